@@ -1,0 +1,349 @@
+"""Benchmark: 3D Gaussian Splatting training iterations/s on the High preset, at full capacity.
+
+Workload "high-300k": the High preset scene (250k ground-truth Gaussians with SH degree 3, 150 views at
+640x480 on a hemisphere with random roll, seed 0) and a model at the preset's 300k-Gaussian cap
+(initGaussiansFromPoints of every true centre plus 50k noisy re-samples). A step is one
+Trainer::step (forward, L1 + D-SSIM loss, backward, Adam) on the next view of the shuffled order, with
+densification finished (the steady phase after refine_stop of the 7000-iteration schedule).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm times K steps with CUDA events on the trainer's stream (inputs resident in HBM), measures
+the same K steps end to end through the C ABI with host buffers (`e2e`: trainer creation from host
+arrays, the steps, the model download), the per-phase device times for the roofline, and the reference
+CPU trainer on a bounded sample of the same workload on the host cores (`cpu_baseline`).
+The reference arm (--impl reference) times the reference's own CPU trainer (oracle/_ref, all host
+threads) on the same workload. With N > 1 (torchrun) every rank trains its own replica (weak scaling;
+the single-scene path has no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "3DGS train it/s + time-to-PSNR (High, 300k); warm-start vs plain, same B200"
+MODEL_CAP = 300_000
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ distributed plumbing
+
+
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while running (start before the timed region, stop after)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.file.flush()
+        self.file.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+
+
+def build_workload(render_on_gpu: bool, seed: int = 0):
+    """The High scene, its ground-truth images and the 300k-Gaussian initial model."""
+    from univeral_3d_reconstruction_system_b200.scenes import dense_init_points, make_scene
+    from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
+
+    t0 = time.time()
+    sc = make_scene("high", seed)
+    st = RasterSettings()
+    if render_on_gpu:
+        from univeral_3d_reconstruction_system_b200 import api
+        imgs = api.renderViewsSh(sc.truth, sc.sh_rest, 3, sc.cameras, st)
+    else:
+        from oracle.binding import Oracle  # the reference arm renders its targets on the host
+        orc = Oracle()
+        imgs = [TrainImage.quantize(orc.render(sc.truth, c, st, sc.sh_rest, 3)) for c in sc.cameras]
+    sc.images = [TrainImage(c, im) for c, im in zip(sc.cameras, imgs)]
+    xyz, rgb = dense_init_points(sc, MODEL_CAP)
+    opt = sc.options()  # TrainOptions::forIterations(7000), max 300k
+    opt.refine_start = opt.iterations + 1  # steady phase: no densification, no opacity reset
+    opt.opacity_reset_interval = 0
+    log(f"workload built in {time.time() - t0:.1f} s")
+    return sc, xyz, rgb, opt
+
+
+def algorithmic_bytes(n: int, v: int, i: int, p: int) -> dict:
+    """Bytes each phase must move at minimum (FP32 parameters, 56 B per Gaussian):
+    project 56N read + 48V record + 4N depth key + 16N rect + 4N radius writes; sort 2 passes of
+    8 B read + 8 B written per item over N (4 passes) and I (2 passes) + emit 8I; forward
+    (4 + 36) I gathers + 20P; loss 27P (render 12, target 3, gradient 12); backward 40I + 36I partial
+    writes + 20P; update 3 x 56N read + 3 x 56N written (params, moments) + 40I partial gathers."""
+    return {
+        "project": 56 * n + 48 * v + 24 * n,
+        "sort": 4 * 16 * n + 2 * 16 * i + 8 * i,
+        "forward": 40 * i + 20 * p,
+        "loss": 27 * p,
+        "backward": 76 * i + 20 * p,
+        "update": 336 * n + 40 * i,
+    }
+
+
+def run_ours(args, dist: Dist) -> dict:
+    from univeral_3d_reconstruction_system_b200 import _lib, api
+
+    L = _lib.load()
+    _lib.check(L.u3dg_set_device(dist.local))
+    sc, xyz, rgb, opt = build_workload(render_on_gpu=True, seed=0)
+    init = api.initGaussiansFromPoints(xyz, rgb)
+    W, K = args.warmup, args.steps
+    total_needed = W + K + args.profile_steps
+    opt.iterations = max(opt.iterations, total_needed + 1)
+    # --- device-timed throughput, inputs resident in HBM
+    t = api.Trainer(init, sc.images, sc.extent, opt)
+    t.step(W)
+    t.synchronize()
+    launches0 = int(L.u3dg_launch_count())
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    clocks.start()
+    ms = t.time_steps(K)
+    clock_info = clocks.stop()
+    launches = int(L.u3dg_launch_count()) - launches0
+    ms = dist.max(ms)
+    # --- per-phase device times (profiled separately: events + a wait per step)
+    t.set_profiling(True)
+    t.step(args.profile_steps)
+    ph = t.phase_times()
+    t.set_profiling(False)
+    stats = t.stats()
+    del t
+    # --- end to end through the C ABI with host buffers
+    dist.barrier()
+    e0 = time.perf_counter()
+    t2 = api.Trainer(init, sc.images, sc.extent, opt)
+    t2.step(K)
+    model = t2.model()
+    st2 = t2.stats()
+    e1 = time.perf_counter()
+    e2e_s = dist.max(e1 - e0)
+    del t2
+    image_bytes = sum(im.rgb.nbytes for im in sc.images)
+    model_bytes = init.size() * 56
+    steps = max(ph["steps"], 1)
+    n, i_avg = ph["gaussians"] / steps, ph["intersections"] / steps
+    p = ph["pixels"] / steps
+    bytes_ = algorithmic_bytes(int(n), int(n), int(i_avg), int(p))
+    phase_ms = {k: ph[f"{k}_ms"] / steps for k in ("project", "sort", "forward", "loss", "backward", "update")}
+    dominant = max(phase_ms, key=phase_ms.get)
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak, peak_src = (float(peaks["hbm_gbs"]), "measured") if "hbm_gbs" in peaks else (6650.0, "fallback")
+    achieved = bytes_[dominant] / (phase_ms[dominant] * 1e-3) / 1e9
+    step_bytes = sum(bytes_.values())
+    per_step_ms = ms / K
+    res = {
+        "value": dist.world * K / (ms * 1e-3),
+        "ms_per_step": per_step_ms,
+        "gpu_launches": launches,
+        "clocks": clock_info,
+        "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "roofline": {
+            "bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} hbm_gbs",
+            "traffic": None, "algorithmic_bytes_per_launch": bytes_[dominant],
+            "step_bytes": step_bytes, "step_achieved_gbs": round(step_bytes / (per_step_ms * 1e-3) / 1e9, 1),
+        },
+        "e2e": {
+            "value": dist.world * K / e2e_s, "unit": "it/s",
+            "h2d_bytes_per_step": int((image_bytes + model_bytes) / K),
+            "d2h_bytes_per_step": int((model.size() * 56) / K + 32),
+            "includes": "trainer creation from host arrays (images + model upload), K steps, model download",
+        },
+        "workload_stats": {"gaussians": int(n), "intersections_per_step": int(i_avg), "pixels": int(p),
+                           "loss_ema": stats.loss, "psnr_ema": stats.psnr, "e2e_psnr_ema": st2.psnr},
+    }
+    return res
+
+
+def cpu_baseline(args, seconds: float = 15.0) -> dict:
+    """The reference CPU trainer (oracle/_ref, built from the reference sources) on a bounded sample of
+    the same workload: one warm-up step, then as many steps as fit in about `seconds`."""
+    from oracle.binding import Reference
+    from univeral_3d_reconstruction_system_b200.types import TrainOptions  # noqa: F401
+
+    if not Reference.available():
+        return {"value": None, "unit": "it/s", "kind": "reference", "cores": os.cpu_count(),
+                "sample": "unavailable: oracle/_ref not built"}
+    ref = Reference()
+    sc, xyz, rgb, opt = build_workload(render_on_gpu=True, seed=0)
+    init = ref.init_from_points(xyz, rgb)
+    threads = ref.pool_threads(0)
+    t = ref.trainer(init, sc.images, sc.extent, opt, threads=0)
+    t0 = time.perf_counter()
+    t.step(1)
+    first = time.perf_counter() - t0
+    k = int(max(2, min(200, seconds / max(first, 1e-3))))
+    t0 = time.perf_counter()
+    t.step(k)
+    dt = time.perf_counter() - t0
+    return {"value": k / dt, "unit": "it/s", "kind": "reference", "cores": threads,
+            "sample": f"{k} steps (after 1 warm-up) of the high-300k workload, reference Trainer with ThreadPool(0)"}
+
+
+def run_reference(args, dist: Dist) -> dict | None:
+    """--impl reference: the reference's own CPU trainer through oracle/_ref on rank 0."""
+    from oracle.binding import Reference
+
+    if dist.rank != 0:
+        return None
+    if not Reference.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libu3dref.so is not built (reference sources absent)"}
+    ref = Reference()
+    sc, xyz, rgb, opt = build_workload(render_on_gpu=False, seed=0)
+    init = ref.init_from_points(xyz, rgb)
+    threads = ref.pool_threads(0)
+    W, K = args.warmup, args.steps
+    opt.iterations = max(opt.iterations, W + K + 1)
+    t = ref.trainer(init, sc.images, sc.extent, opt, threads=0)
+    t.step(W)
+    t0 = time.perf_counter()
+    t.step(K)
+    dt = time.perf_counter() - t0
+    v = K / dt
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "it/s", "n_gpus": dist.world, "steps": K,
+            "warmup": W, "ms_per_step": dt * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config(args, dist),
+            "cpu_baseline": {"value": v, "unit": "it/s", "kind": "reference", "cores": threads,
+                             "sample": f"{K} steps after {W} warm-up steps of the high-300k workload"},
+            "e2e": {"value": v, "unit": "it/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def config(args, dist: Dist) -> dict:
+    return {"workload": "high-300k", "scene": "High preset (seed 0): 250k GT Gaussians, SH3, 150 views 640x480",
+            "model_gaussians": MODEL_CAP, "resolution": "640x480", "views": 150, "tile": 16,
+            "phase": "steady (densification finished)", "parallelism": f"replicas x{dist.world}",
+            "l2": "inputs larger than L2: per step the model, Adam moments and raster buffers (~0.3 GB) "
+                  "exceed the 126 MB L2"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, dist)
+            if out is not None:
+                print(json.dumps(out), flush=True)
+            return
+        res = run_ours(args, dist)
+        line = {"metric": METRIC, "value": res["value"], "unit": "it/s", "n_gpus": dist.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config(args, dist), "roofline": res["roofline"], "e2e": res["e2e"],
+                "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "phase_ms": res["phase_ms"],
+                "workload_stats": res["workload_stats"]}
+        if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
+        if dist.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -146,6 +146,8 @@ typedef struct u3dg_adam u3dg_adam;
 const char *u3dg_last_error(void);
 /* U3DG_ABI_VERSION of the loaded library. */
 int u3dg_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process (all devices, all objects). */
+uint64_t u3dg_launch_count(void);
 /* Number of CUDA devices visible (0 without a GPU; never fails). */
 int u3dg_device_count(void);
 /* Selects the CUDA device used by objects created afterwards on this thread. */
@@ -230,6 +232,18 @@ void u3dg_rasterizer_destroy(u3dg_rasterizer *r);
 int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_t n, int tiles_x, int tiles_y,
                    int *offsets, int *list, size_t list_capacity, size_t *list_length);
 
+/* Trainer::densifyAndPrune (engine/src/splat/Trainer.cpp:105-169) on a given state, through the same
+ * GPU code path the trainer uses. model, adam_m and adam_v are host arrays with room for `capacity`
+ * Gaussians of which model->count are valid; they are densified in place and *count gets the new
+ * size (U3DG_ERR_CAPACITY if it exceeds capacity). grad_accum / grad_count (model->count entries) are
+ * the densification statistics. Split samples come from std::mt19937(seed) through
+ * std::normal_distribution<float>, drawn in the reference's order. counts3 (may be NULL) gets the
+ * numbers of pruned, cloned and split Gaussians. */
+int u3dg_densify_and_prune(u3dg_model *model, u3dg_model *adam_m, u3dg_model *adam_v, const float *grad_accum,
+                           const int *grad_count, size_t capacity, float scene_extent,
+                           const u3dg_train_options *options, int opacity_was_reset, unsigned int seed, size_t *count,
+                           int *counts3);
+
 /* ------------------------------------------------------------------ loss */
 
 /* photometricLoss (engine/include/u3d/splat/Loss.h:18-19, engine/src/splat/Loss.cpp:47-184):
@@ -278,6 +292,11 @@ int u3dg_read_splat_ply(const char *path, u3dg_model *out, size_t capacity, size
  * Rasterizer.cpp:189-194); used to render the synthetic scenes' ground truth. */
 int u3dg_render_sh(const u3dg_model *model, const float *sh_rest, int degree, const u3dg_camera *camera,
                    const u3dg_raster_settings *settings, float *rgb);
+/* u3dg_render_sh over `count` cameras with the model uploaded once; every view is quantised like
+ * TrainImage::quantize (engine/src/splat/Trainer.cpp:10-16: lround(clamp(v, 0, 1) * 255)) into
+ * rgb8, views back to back (sum of width*height*3 bytes). */
+int u3dg_render_views_sh(const u3dg_model *model, const float *sh_rest, int degree, const u3dg_camera *cameras,
+                         int count, const u3dg_raster_settings *settings, uint8_t *rgb8);
 
 #ifdef __cplusplus
 }

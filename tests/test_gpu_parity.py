@@ -1,0 +1,366 @@
+"""GPU parity: every stage of the CUDA path against the CPU oracle on identical seeded inputs.
+
+Bars (written per test): tile lists and their order bit-exact; projection bit-exact except where
+glibc's expf differs from the correctly rounded exp (counted, must stay rare); rendered images within
+1e-5 absolute per channel; loss values and gradients within float rounding of the oracle;
+per-parameter gradients within 1e-4 relative (with a floor of 1e-3 of the group's largest value);
+Adam bit-exact; densification bit-exact in structure.
+"""
+import numpy as np
+import pytest
+
+from helpers import fd_setup, grad_close, make_camera, orbit_camera, random_model, rel_l2
+from univeral_3d_reconstruction_system_b200.scenes import make_scene, render_targets
+from univeral_3d_reconstruction_system_b200.types import GaussianModel, RasterSettings, TrainImage, TrainOptions, logit
+
+pytestmark = pytest.mark.gpu
+
+GROUPS = ("means", "scales", "quats", "opacities", "colors")
+
+
+@pytest.fixture(scope="module")
+def tiny_scene(oracle):
+    sc = make_scene("tiny", 0)
+    st = RasterSettings()
+    render_targets(sc, lambda m, sh, d, c: oracle.render(m, c, st, sh, d))
+    return sc
+
+
+def _views(sc, k=4):
+    return sc.cameras[:k]
+
+
+# ------------------------------------------------------------------ projection
+
+
+def test_projection_matches_oracle(u3dg, oracle, tiny_scene):
+    sc = tiny_scene
+    st = RasterSettings()
+    r = u3dg.Rasterizer()
+    for cam in _views(sc, 6):
+        r.forward(sc.truth, cam, st)
+        g = r.projection()
+        o = oracle.raster(4)
+        o.forward(sc.truth, cam, st)
+        p = o.projection()
+        vis_g, vis_o = g["radius"] > 0, p["radius"] > 0
+        # Visibility / radius / tile rectangle: equal except for glibc-expf ulp cases (rare).
+        mism = np.count_nonzero((g["radius"] != p["radius"]) | np.any(g["rect"] != p["rect"], axis=1))
+        assert mism <= max(1, sc.truth.size() // 2000), mism
+        both = vis_g & vis_o
+        assert both.sum() > 100
+        for key in ("mean2d", "depth"):
+            np.testing.assert_array_equal(g[key][both], p[key][both])  # no exp on this path: bit-exact
+        for key in ("conic", "cov2d", "rgb", "alpha"):
+            np.testing.assert_allclose(g[key][both], p[key][both], rtol=2e-6, atol=1e-7)
+        np.testing.assert_array_equal(g["flags"][both], p["flags"][both])
+
+
+def test_closed_form_projection(u3dg):
+    """splat_projection_matches_closed_form (test_splat.cpp:153-191) on the GPU."""
+    sx, sy, angle = 0.05, 0.12, 0.6
+    m = GaussianModel(np.array([[0, 0, 3]], np.float32), np.log(np.array([[sx, sy, 0.02]], np.float32)),
+                      np.array([[np.cos(angle / 2), 0, 0, np.sin(angle / 2)]], np.float32),
+                      np.array([logit(0.5)], np.float32), np.full((1, 3), 0.5 / 0.28209479177387814, np.float32))
+    cam = make_camera(201, 201, 300.0)
+    st = RasterSettings(min_alpha=0.0, min_transmittance=0.0)
+    rgb = u3dg.Rasterizer().forward(m, cam, st)[..., 0].astype(np.float64)
+    ys, xs = np.mgrid[0:201, 0:201]
+    w = rgb.sum()
+    mx, my = (rgb * xs).sum() / w, (rgb * ys).sum() / w
+    a = (rgb * (xs - mx) ** 2).sum() / w
+    b = (rgb * (xs - mx) * (ys - my)).sum() / w
+    c = (rgb * (ys - my) ** 2).sum() / w
+    k2, ca, sa = (300.0 / 3.0) ** 2, np.cos(angle), np.sin(angle)
+    assert abs(mx - 100) < 0.01 and abs(my - 100) < 0.01
+    assert abs(a - (k2 * (ca * ca * sx * sx + sa * sa * sy * sy) + 0.3)) < 0.2
+    assert abs(b - k2 * ca * sa * (sx * sx - sy * sy)) < 0.2
+    assert abs(c - (k2 * (sa * sa * sx * sx + ca * ca * sy * sy) + 0.3)) < 0.2
+
+
+# ------------------------------------------------------------------ binning
+
+
+def _check_bins(u3dg, oracle, depth, radius, rect, tx, ty):
+    og, ol = oracle.bin_tiles(depth, radius, rect, tx, ty)
+    gg, gl = u3dg.binTiles(depth, radius, rect, tx, ty)
+    np.testing.assert_array_equal(gg, og)
+    np.testing.assert_array_equal(gl, ol)
+    return len(ol)
+
+
+def test_tile_lists_bit_exact_on_identical_records(u3dg, oracle, tiny_scene):
+    """Tile offsets and lists (including the depth order inside every tile) equal the oracle's
+    binTiles restatement exactly, given the same projected records."""
+    sc = tiny_scene
+    st = RasterSettings()
+    for cam in _views(sc, 8):
+        o = oracle.raster(4)
+        o.forward(sc.truth, cam, st)
+        p = o.projection()
+        tx, ty = (cam.width + 15) // 16, (cam.height + 15) // 16
+        assert _check_bins(u3dg, oracle, p["depth"], p["radius"], p["rect"], tx, ty) > 0
+
+
+def test_tile_lists_edge_cases(u3dg, oracle):
+    rng = np.random.default_rng(5)
+    # Empty input, all invisible, and a single tile.
+    _check_bins(u3dg, oracle, np.zeros(0, np.float32), np.zeros(0, np.int32), np.zeros((0, 4), np.int32), 3, 2)
+    n = 50
+    _check_bins(u3dg, oracle, rng.uniform(1, 5, n).astype(np.float32), np.zeros(n, np.int32),
+                np.zeros((n, 4), np.int32), 3, 2)
+    rect1 = np.tile(np.array([0, 0, 1, 1], np.int32), (n, 1))
+    _check_bins(u3dg, oracle, rng.uniform(1, 5, n).astype(np.float32), np.ones(n, np.int32), rect1, 1, 1)
+    # Many exact depth ties (ties keep index order), random rectangles, > 256 tiles (two sort passes),
+    # and more items than one sort block.
+    for n, tx, ty, levels in ((5000, 40, 30, 7), (70000, 17, 19, 1000), (3000, 300, 2, 3)):
+        depth = rng.integers(1, levels + 1, n).astype(np.float32) * np.float32(0.5)
+        x0 = rng.integers(0, tx, n)
+        y0 = rng.integers(0, ty, n)
+        x1 = np.minimum(tx, x0 + rng.integers(1, 4, n))
+        y1 = np.minimum(ty, y0 + rng.integers(1, 4, n))
+        rect = np.stack([x0, y0, x1, y1], 1).astype(np.int32)
+        radius = np.where(rng.uniform(size=n) < 0.8, 5, 0).astype(np.int32)
+        _check_bins(u3dg, oracle, depth, radius, rect, tx, ty)
+
+
+# ------------------------------------------------------------------ compositing forward
+
+
+@pytest.mark.parametrize("tile", [16, 8, 32, 64])
+def test_forward_image_matches_oracle(u3dg, oracle, tiny_scene, tile):
+    sc = tiny_scene
+    st = RasterSettings(tile_size=tile, background=(0.1, 0.2, 0.3))
+    r = u3dg.Rasterizer()
+    for cam in _views(sc, 3):
+        img = r.forward(sc.truth, cam, st)
+        o = oracle.raster(4)
+        ref = o.forward(sc.truth, cam, st)
+        assert np.max(np.abs(img - ref)) <= 1e-5
+        ft, nc = r.pixel_state()
+        oft, onc = o.pixel_state()
+        np.testing.assert_array_equal(nc, onc)
+        assert np.max(np.abs(ft - oft)) <= 1e-5
+        go, gl = r.tiles()
+        oo, ol = o.tiles()
+        np.testing.assert_array_equal(go, oo)
+        np.testing.assert_array_equal(gl, ol)
+
+
+def test_forward_dense_scene(u3dg, oracle):
+    """A denser model (many overlapping, early-terminating pixels) at 160x120."""
+    sc = make_scene("small", 1)
+    st = RasterSettings()
+    img = u3dg.Rasterizer().forward(sc.truth, sc.cameras[0], st)
+    ref = oracle.render(sc.truth, sc.cameras[0], st)
+    assert np.max(np.abs(img - ref)) <= 1e-5
+
+
+# ------------------------------------------------------------------ loss
+
+
+@pytest.mark.parametrize("lam", [0.2, 1.0, 0.0])
+def test_loss_matches_oracle(u3dg, oracle, lam):
+    rng = np.random.default_rng(3)
+    for W, H in ((21, 17), (96, 72), (333, 47)):
+        target = rng.uniform(0, 1, (H, W, 3)).astype(np.float32)
+        render = (0.5 * target + 0.5 * rng.uniform(0, 1, (H, W, 3))).astype(np.float32)
+        gv, gg = u3dg.photometricLoss(render, target, W, H, lam)
+        ov, og = oracle.photometric_loss(render, target, W, H, lam)
+        assert abs(gv.l1 - ov.l1) <= 1e-7 * max(1.0, abs(ov.l1))
+        assert abs(gv.ssim - ov.ssim) <= 1e-6
+        assert abs(gv.total - ov.total) <= 1e-6
+        np.testing.assert_allclose(gg.reshape(-1), og.reshape(-1), rtol=1e-5, atol=1e-9)
+
+
+def test_ssim_gradient_finite_differences(u3dg):
+    """ssim_loss_gradient (test_splat.cpp:193-225) on the GPU: pure D-SSIM, every 7th pixel."""
+    W, H = 21, 17
+    rng = np.random.default_rng(3)
+    target = rng.uniform(0, 1, (H, W, 3)).astype(np.float32)
+    render = (0.5 * target + 0.5 * rng.uniform(0, 1, (H, W, 3))).astype(np.float32)
+    _, grad = u3dg.photometricLoss(render, target, W, H, 1.0)
+    flat = render.reshape(-1)
+    num, ana = [], []
+    eps = 1e-3
+    for k in range(0, flat.size, 7):
+        o = flat[k]
+        flat[k] = o + eps
+        lp = u3dg.photometricLoss(render, target, W, H, 1.0)[0].total
+        flat[k] = o - eps
+        lm = u3dg.photometricLoss(render, target, W, H, 1.0)[0].total
+        flat[k] = o
+        num.append((lp - lm) / (2 * eps))
+        ana.append(grad.reshape(-1)[k])
+    assert rel_l2(ana, num) < 0.02
+    same = u3dg.photometricLoss(target, target, W, H, 0.2)[0]
+    assert abs(same.ssim - 1.0) < 1e-4 and abs(same.total) < 1e-4
+
+
+def test_psnr(u3dg, oracle):
+    rng = np.random.default_rng(0)
+    a = rng.uniform(size=10000).astype(np.float32)
+    b = (a + rng.normal(0, 0.01, a.size)).astype(np.float32)
+    assert abs(u3dg.psnr(a, b) - oracle.psnr(a, b)) < 1e-4
+    assert u3dg.psnr(a, a) == 99.0
+
+
+# ------------------------------------------------------------------ backward
+
+
+def _backward_both(u3dg, oracle, model, cam, st, w):
+    r = u3dg.Rasterizer()
+    r.forward(model, cam, st)
+    ndc = np.zeros(model.size(), np.float32)
+    g = r.backward(model, w, None, ndc)
+    o = oracle.raster(4)
+    o.forward(model, cam, st)
+    og, ondc = o.backward(w)
+    return g, ndc, og, ondc
+
+
+def test_backward_matches_oracle(u3dg, oracle, tiny_scene):
+    sc = tiny_scene
+    st = RasterSettings()
+    rng = np.random.default_rng(11)
+    for cam in _views(sc, 3):
+        w = rng.uniform(-1, 1, (cam.height, cam.width, 3)).astype(np.float32)
+        g, ndc, og, ondc = _backward_both(u3dg, oracle, sc.truth, cam, st, w)
+        for name in GROUPS:
+            ok, worst = grad_close(getattr(g, name), getattr(og, name), rel=1e-4)
+            assert ok, (name, worst)
+        ok, worst = grad_close(ndc, ondc, rel=1e-4)
+        assert ok, ("ndc", worst)
+
+
+def test_backward_tile64_matches_oracle(u3dg, oracle):
+    model, cam, st, rng = fd_setup()
+    w = rng.uniform(-1, 1, (cam.height, cam.width, 3)).astype(np.float32)
+    g, ndc, og, ondc = _backward_both(u3dg, oracle, model, cam, st, w)
+    for name in GROUPS:
+        ok, worst = grad_close(getattr(g, name), getattr(og, name), rel=1e-4)
+        assert ok, (name, worst)
+
+
+def test_gradients_match_finite_differences(u3dg):
+    """splat_gradients_match_finite_differences (test_splat.cpp:110-151) on the GPU: central
+    differences of a random-weighted pixel sum over every parameter; relative L2 error < 0.02."""
+    model, cam, st, rng = fd_setup()
+    r = u3dg.Rasterizer()
+    rgb = r.forward(model, cam, st)
+    w = rng.uniform(-1, 1, rgb.shape).astype(np.float32)
+    g = r.backward(model, w)
+
+    def loss(m):
+        return float(np.sum(w.astype(np.float64) * u3dg.Rasterizer().forward(m, cam, st).astype(np.float64)))
+
+    for name in GROUPS:
+        p = getattr(model, name).reshape(-1)
+        num = np.zeros(p.size)
+        for k in range(p.size):
+            o = p[k]
+            p[k] = o + np.float32(1e-3)
+            lp = loss(model)
+            p[k] = o - np.float32(1e-3)
+            lm = loss(model)
+            p[k] = o
+            num[k] = (lp - lm) / 2e-3
+        assert rel_l2(getattr(g, name).reshape(-1), num) < 0.02, name
+
+
+# ------------------------------------------------------------------ Adam, densify
+
+
+def test_adam_bit_exact(u3dg, oracle):
+    rng = np.random.default_rng(2)
+    n = 1000
+    p = GaussianModel(*(rng.normal(size=s).astype(np.float32) for s in ((n, 3), (n, 3), (n, 4), (n,), (n, 3))))
+    po = p.copy()
+    m, v = GaussianModel.zeros(n), GaussianModel.zeros(n)
+    adam = u3dg.Adam()
+    adam.reset(n)
+    lr = TrainOptions().lr
+    for step in range(1, 6):
+        g = GaussianModel(*(rng.normal(size=s).astype(np.float32) for s in ((n, 3), (n, 3), (n, 4), (n,), (n, 3))))
+        adam.step(p, g, lr)
+        oracle.adam_step(po, g, m, v, step, lr)
+        np.testing.assert_array_equal(p.flat(), po.flat())
+    gm, gv = adam.moments()
+    np.testing.assert_array_equal(gm.flat(), m.flat())
+    np.testing.assert_array_equal(gv.flat(), v.flat())
+
+
+@pytest.mark.parametrize("case", ["budget", "no_budget", "after_reset", "one_slot"])
+def test_densify_matches_oracle(u3dg, oracle, case):
+    rng = np.random.default_rng(4)
+    n = 3000
+    model = GaussianModel(rng.uniform(-1, 1, (n, 3)).astype(np.float32),
+                          rng.normal(-4.0, 1.0, (n, 3)).astype(np.float32),
+                          rng.normal(size=(n, 4)).astype(np.float32),
+                          rng.normal(-2.0, 2.5, n).astype(np.float32),
+                          rng.normal(size=(n, 3)).astype(np.float32))
+    m = GaussianModel(*(rng.normal(size=a.shape).astype(np.float32) for a in
+                        (model.means, model.scales, model.quats, model.opacities, model.colors)))
+    v = GaussianModel(*(np.abs(rng.normal(size=a.shape)).astype(np.float32) for a in
+                        (model.means, model.scales, model.quats, model.opacities, model.colors)))
+    acc = np.abs(rng.normal(0, 4e-3, n)).astype(np.float32)
+    cnt = rng.integers(0, 20, n).astype(np.int32)
+    o = TrainOptions(max_gaussians={"budget": n + 400, "no_budget": n, "after_reset": 2 * n,
+                                    "one_slot": n + 1}[case])
+    extent = 0.8
+    reset = case == "after_reset"
+    gm, gmm, gvv, gc = u3dg.densifyAndPrune(model, m, v, acc, cnt, extent, o, reset, 1234)
+    om, omm, ovv, oc = oracle.densify(model, m, v, acc, cnt, extent, o, reset, 1234)
+    np.testing.assert_array_equal(gc, oc)
+    assert gm.size() == om.size()
+    for name in GROUPS:
+        np.testing.assert_allclose(getattr(gm, name), getattr(om, name), rtol=2e-6, atol=1e-7)
+        np.testing.assert_array_equal(getattr(gmm, name), getattr(omm, name))
+        np.testing.assert_array_equal(getattr(gvv, name), getattr(ovv, name))
+
+
+# ------------------------------------------------------------------ trainer
+
+
+def test_trainer_matches_oracle_trajectory(u3dg, oracle, tiny_scene):
+    """Same scene, same options, same view order: the GPU trainer's loss / PSNR stay on the oracle's
+    trajectory (gradient sums differ in rounding only) and the final evaluatePsnr agrees to 0.1 dB."""
+    sc = tiny_scene
+    init = oracle.init_from_points(sc.init_xyz, sc.init_rgb)
+    opt = sc.options()
+    g = u3dg.Trainer(init, sc.images, sc.extent, opt)
+    o = oracle.trainer(init, sc.images, sc.extent, opt, threads=8)
+    for _ in range(3):
+        g.step(100)
+        o.step(100)
+        gs, os_ = g.stats(), o.stats()
+        assert gs.iteration == os_.iteration
+        assert abs(gs.psnr - os_.psnr) < 0.1, (gs.psnr, os_.psnr)
+        assert abs(gs.loss - os_.loss) < 2e-3 * max(1.0, os_.loss)
+    assert g.done()
+    assert abs(g.size() - o.size()) <= max(2, o.size() // 100)
+    assert abs(g.evaluatePsnr() - o.evaluate_psnr()) < 0.1
+
+
+def test_training_recovers_a_synthetic_scene(u3dg, oracle):
+    """training_recovers_a_synthetic_scene (test_splat.cpp:227-268) on the GPU."""
+    rng = np.random.default_rng(11)
+    truth = random_model(300, rng, 1.0, 0.0, 0.03, 0.12)
+    truth.opacities[:] = logit(0.8)
+    st = RasterSettings()
+    images = []
+    for k in range(16):
+        cam = orbit_camera(96, 72, 80.0, 6.2831853 * k / 16.0, 4.0, -1.0 + 0.15 * (k % 4))
+        images.append(TrainImage(cam, TrainImage.quantize(oracle.render(truth, cam, st))))
+    xyz = np.stack([truth.means[i] + rng.normal(0, 0.08, 3) for i in range(0, 300, 2)]).astype(np.float32)
+    init = u3dg.initGaussiansFromPoints(xyz, np.full_like(xyz, 0.5))
+    opt = TrainOptions.for_iterations(1500)
+    opt.max_gaussians = 4000
+    t = u3dg.Trainer(init, images, 4.4, opt)
+    before = t.evaluatePsnr()
+    while not t.done():
+        t.step(100)
+    after = t.evaluatePsnr()
+    assert after > before + 8.0, (before, after)
+    assert after > 26.0, after
+    assert t.model().size() != init.size()

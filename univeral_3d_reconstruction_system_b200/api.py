@@ -1,0 +1,373 @@
+"""Python mirror of the reference's splat API over the CUDA library (libu3dg.so).
+
+Same classes, method names and argument meaning as engine/include/u3d/splat:
+  Trainer             Trainer.h:47-93     (step, done, iteration, model, stats, images, evaluatePsnr, render)
+  Rasterizer          Rasterizer.h:38-90  (forward, backward, radii)
+  photometricLoss     Loss.h:18-19
+  psnr                Loss.h:21
+  Adam                Adam.h:18-31
+  initGaussiansFromPoints  GaussianModel.h:41
+  writeSplatPly / readSplatPly  SplatPly.h:12-24
+Errors raise U3dgError (the reference has no error channel besides bool returns for PLY I/O;
+writeSplatPly / readSplatPly keep that: they return False and set .error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._lib import U3dgError, check, load
+from .types import GaussianModel, LossValue, RasterSettings, RenderCamera, TrainImage, TrainOptions, TrainStats, \
+    images_struct
+
+
+def _cam(camera):
+    return camera.struct() if hasattr(camera, "struct") else camera
+
+
+def _settings(settings):
+    return (settings or RasterSettings()).struct() if not isinstance(settings, _abi.RasterSettings) else settings
+
+
+class Trainer:
+    """GPU drop-in for u3d::Trainer. `pool` is accepted for API compatibility and ignored."""
+
+    def __init__(self, initial: GaussianModel, images, scene_extent: float, options: TrainOptions | None = None,
+                 pool=None):
+        L = load()
+        self._images = list(images)
+        self._options = options or TrainOptions()
+        arr, keep = images_struct(self._images)
+        iv = initial.view()
+        opt = self._options.struct()
+        h = C.c_void_p()
+        check(L.u3dg_trainer_create(C.byref(iv), arr, len(self._images), float(scene_extent), C.byref(opt),
+                                    C.byref(h)))
+        self._h = h
+        del keep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            load().u3dg_trainer_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def step(self, count: int = 1) -> None:
+        check(load().u3dg_trainer_step(self._h, count))
+
+    def done(self) -> bool:
+        d = C.c_int()
+        check(load().u3dg_trainer_done(self._h, C.byref(d)))
+        return bool(d.value)
+
+    def iteration(self) -> int:
+        it = C.c_int()
+        check(load().u3dg_trainer_iteration(self._h, C.byref(it)))
+        return it.value
+
+    def size(self) -> int:
+        n = C.c_size_t()
+        check(load().u3dg_trainer_size(self._h, C.byref(n)))
+        return int(n.value)
+
+    def model(self) -> GaussianModel:
+        n = self.size()
+        m = GaussianModel.zeros(n)
+        v = m.view()
+        cnt = C.c_size_t()
+        check(load().u3dg_trainer_download(self._h, C.byref(v), n, C.byref(cnt)))
+        return m
+
+    def stats(self) -> TrainStats:
+        s = _abi.TrainStats()
+        check(load().u3dg_trainer_stats(self._h, C.byref(s)))
+        return TrainStats(s.iteration, s.loss, s.psnr, int(s.gaussians))
+
+    def images(self):
+        return self._images
+
+    def evaluatePsnr(self) -> float:
+        p = C.c_float()
+        check(load().u3dg_trainer_eval_psnr(self._h, C.byref(p)))
+        return float(p.value)
+
+    evaluate_psnr = evaluatePsnr
+
+    def render(self, camera: RenderCamera) -> np.ndarray:
+        cs = _cam(camera)
+        rgb = np.zeros((cs.height, cs.width, 3), np.float32)
+        check(load().u3dg_trainer_render(self._h, C.byref(cs), _abi.fptr(rgb)))
+        return rgb
+
+    # -- measurement helpers (no reference counterpart)
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(load().u3dg_trainer_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def synchronize(self) -> None:
+        check(load().u3dg_trainer_synchronize(self._h))
+
+    def time_steps(self, count: int) -> float:
+        """Device milliseconds of `count` steps (CUDA events on the trainer's stream)."""
+        ms = C.c_float()
+        check(load().u3dg_trainer_time_steps(self._h, count, C.byref(ms)))
+        return float(ms.value)
+
+    def set_profiling(self, enable: bool) -> None:
+        check(load().u3dg_trainer_set_profiling(self._h, 1 if enable else 0))
+
+    def phase_times(self) -> dict:
+        t = _abi.PhaseTimes()
+        check(load().u3dg_trainer_phase_times(self._h, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+
+class Rasterizer:
+    """GPU drop-in for u3d::Rasterizer (forward keeps the state backward needs)."""
+
+    def __init__(self, pool=None):
+        h = C.c_void_p()
+        check(load().u3dg_rasterizer_create(C.byref(h)))
+        self._h = h
+        self._n = 0
+        self._cam = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            load().u3dg_rasterizer_destroy(h)
+            self._h = None
+
+    def forward(self, model: GaussianModel, camera, settings: RasterSettings | None = None) -> np.ndarray:
+        cs, ss = _cam(camera), _settings(settings)
+        rgb = np.zeros((cs.height, cs.width, 3), np.float32)
+        mv = model.view()
+        check(load().u3dg_rasterizer_forward(self._h, C.byref(mv), C.byref(cs), C.byref(ss), _abi.fptr(rgb)))
+        self._n, self._cam, self._ss = model.size(), cs, ss
+        return rgb
+
+    def backward(self, model: GaussianModel, dl_drgb: np.ndarray, grads: GaussianModel | None = None,
+                 mean2d_grad_ndc: np.ndarray | None = None):
+        """ADDS dL/dparams into `grads` (zeros if None) and |dL/dmean2d| into mean2d_grad_ndc; returns grads."""
+        g = grads if grads is not None else GaussianModel.zeros(model.size())
+        mv, gv = model.view(), g.view()
+        dl = np.ascontiguousarray(dl_drgb, np.float32)
+        ndc = _abi.fptr(mean2d_grad_ndc) if mean2d_grad_ndc is not None else None
+        check(load().u3dg_rasterizer_backward(self._h, C.byref(mv), _abi.fptr(dl), C.byref(gv), ndc))
+        return g
+
+    def radii(self) -> np.ndarray:
+        out = np.zeros(self._n, np.int32)
+        check(load().u3dg_rasterizer_radii(self._h, _abi.iptr(out), self._n))
+        return out
+
+    def projection(self) -> dict:
+        n = self._n
+        out = dict(mean2d=np.zeros((n, 2), np.float32), conic=np.zeros((n, 3), np.float32),
+                   cov2d=np.zeros((n, 3), np.float32), depth=np.zeros(n, np.float32), rgb=np.zeros((n, 3), np.float32),
+                   alpha=np.zeros(n, np.float32), rect=np.zeros((n, 4), np.int32), flags=np.zeros(n, np.uint8))
+        check(load().u3dg_rasterizer_projection(self._h, n, *(_abi.fptr(out[k]) for k in
+                                                              ("mean2d", "conic", "cov2d", "depth", "rgb", "alpha")),
+                                                _abi.iptr(out["rect"]), out["flags"].ctypes.data_as(_abi.u8p)))
+        out["radius"] = self.radii()
+        return out
+
+    def tiles(self):
+        tx, ty, L = C.c_int(), C.c_int(), C.c_size_t()
+        check(load().u3dg_rasterizer_tiles(self._h, C.byref(tx), C.byref(ty), None, 0, None, 0, C.byref(L)))
+        offsets = np.zeros(tx.value * ty.value + 1, np.int32)
+        lst = np.zeros(max(L.value, 1), np.int32)
+        check(load().u3dg_rasterizer_tiles(self._h, None, None, _abi.iptr(offsets), offsets.size, _abi.iptr(lst),
+                                           lst.size, C.byref(L)))
+        return offsets, lst[: L.value]
+
+    def pixel_state(self):
+        P = self._cam.width * self._cam.height
+        ft = np.zeros(P, np.float32)
+        nc = np.zeros(P, np.int32)
+        check(load().u3dg_rasterizer_pixel_state(self._h, _abi.fptr(ft), _abi.iptr(nc), P))
+        return ft, nc
+
+
+def binTiles(depth, radius, rect, tiles_x: int, tiles_y: int):
+    """GPU tile binning of given projected records (Rasterizer::binTiles); returns (offsets, list)."""
+    depth = np.ascontiguousarray(depth, np.float32)
+    radius = np.ascontiguousarray(radius, np.int32)
+    rect = np.ascontiguousarray(rect, np.int32).reshape(-1)
+    offsets = np.zeros(tiles_x * tiles_y + 1, np.int32)
+    L = C.c_size_t()
+    check(load().u3dg_bin_tiles(_abi.fptr(depth), _abi.iptr(radius), _abi.iptr(rect), depth.size, tiles_x, tiles_y,
+                                _abi.iptr(offsets), None, 0, C.byref(L)))
+    lst = np.zeros(max(L.value, 1), np.int32)
+    check(load().u3dg_bin_tiles(_abi.fptr(depth), _abi.iptr(radius), _abi.iptr(rect), depth.size, tiles_x, tiles_y,
+                                _abi.iptr(offsets), _abi.iptr(lst), lst.size, C.byref(L)))
+    return offsets, lst[: L.value]
+
+
+def photometricLoss(render: np.ndarray, target: np.ndarray, width: int, height: int, ssim_lambda: float):
+    """Returns (LossValue, dLoss/drender) (Loss.h:18-19)."""
+    r = np.ascontiguousarray(render, np.float32).reshape(-1)
+    t = np.ascontiguousarray(target, np.float32).reshape(-1)
+    g = np.zeros_like(r)
+    out = _abi.LossValue()
+    check(load().u3dg_photometric_loss(_abi.fptr(r), _abi.fptr(t), width, height, float(ssim_lambda), _abi.fptr(g),
+                                       C.byref(out)))
+    return LossValue(out.total, out.l1, out.ssim), g.reshape(np.shape(render))
+
+
+def psnr(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.ascontiguousarray(a, np.float32).reshape(-1)
+    b = np.ascontiguousarray(b, np.float32).reshape(-1)
+    out = C.c_float()
+    check(load().u3dg_psnr(_abi.fptr(a), _abi.fptr(b), a.size, C.byref(out)))
+    return float(out.value)
+
+
+class Adam:
+    """u3d::Adam with the moments on the GPU (params are host arrays updated in place)."""
+
+    def __init__(self):
+        self._h = None
+        self._n = 0
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            load().u3dg_adam_destroy(self._h)
+            self._h = None
+
+    def reset(self, n: int) -> None:
+        self.__del__()
+        h = C.c_void_p()
+        check(load().u3dg_adam_create(n, C.byref(h)))
+        self._h, self._n = h, n
+
+    def step(self, params: GaussianModel, grads: GaussianModel, lr) -> None:
+        pv, gv = params.view(), grads.view()
+        lrs = lr.struct()
+        check(load().u3dg_adam_step(self._h, C.byref(pv), C.byref(gv), C.byref(lrs)))
+
+    def compact(self, keep) -> None:
+        k = np.ascontiguousarray(keep, np.uint8)
+        check(load().u3dg_adam_compact(self._h, k.ctypes.data_as(_abi.u8p), k.size))
+        self._n = int(np.count_nonzero(k))
+
+    def grow(self, count: int) -> None:
+        check(load().u3dg_adam_grow(self._h, count))
+        self._n += count
+
+    def resetOpacityMoments(self) -> None:
+        check(load().u3dg_adam_reset_opacity_moments(self._h))
+
+    def moments(self):
+        m, v = GaussianModel.zeros(self._n), GaussianModel.zeros(self._n)
+        mv, vv = m.view(), v.view()
+        check(load().u3dg_adam_moments(self._h, C.byref(mv), C.byref(vv)))
+        return m, v
+
+
+def densifyAndPrune(model: GaussianModel, m: GaussianModel, v: GaussianModel, grad_accum, grad_count, extent: float,
+                    options: TrainOptions, opacity_was_reset: bool, seed: int):
+    """Trainer::densifyAndPrune on a given state (GPU path of the trainer). Returns (model, m, v, counts)."""
+    cap = max(options.max_gaussians, model.size())
+    bufs = [GaussianModel.zeros(cap) for _ in range(3)]
+    for dst, src in zip(bufs, (model, m, v)):
+        for name, _ in _abi.GROUPS:
+            getattr(dst, name)[: src.size()] = getattr(src, name)
+    views = [b.view() for b in bufs]
+    for vw in views:
+        vw.count = model.size()
+    count = C.c_size_t()
+    counts = np.zeros(3, np.int32)
+    opt = options.struct()
+    check(load().u3dg_densify_and_prune(C.byref(views[0]), C.byref(views[1]), C.byref(views[2]),
+                                        _abi.fptr(np.ascontiguousarray(grad_accum, np.float32)),
+                                        _abi.iptr(np.ascontiguousarray(grad_count, np.int32)), cap, float(extent),
+                                        C.byref(opt), int(bool(opacity_was_reset)), seed, C.byref(count),
+                                        _abi.iptr(counts)))
+    k = count.value
+    out = [GaussianModel(*(getattr(b, name)[:k].copy() for name, _ in _abi.GROUPS)) for b in bufs]
+    return out[0], out[1], out[2], counts
+
+
+def initGaussiansFromPoints(xyz: np.ndarray, rgb: np.ndarray | None = None) -> GaussianModel:
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1)
+    n = x.size // 3
+    out = GaussianModel.zeros(n)
+    v = out.view()
+    rp = _abi.fptr(np.ascontiguousarray(rgb, np.float32).reshape(-1)) if rgb is not None else None
+    check(load().u3dg_init_gaussians_from_points(_abi.fptr(x), rp, n, C.byref(v)))
+    return out
+
+
+class PlyResult:
+    def __init__(self):
+        self.error = ""
+
+
+def writeSplatPly(path: str, model: GaussianModel, result: PlyResult | None = None) -> bool:
+    v = model.view()
+    st = load().u3dg_write_splat_ply(str(path).encode(), C.byref(v))
+    if st != _abi.OK and result is not None:
+        result.error = load().u3dg_last_error().decode()
+    return st == _abi.OK
+
+
+def readSplatPly(path: str, result: PlyResult | None = None):
+    """Returns (model or None, is_splat)."""
+    L = load()
+    n = C.c_size_t()
+    is_splat = C.c_int()
+    st = L.u3dg_read_splat_ply(str(path).encode(), None, 0, C.byref(n), C.byref(is_splat))
+    if st != _abi.OK:
+        if result is not None:
+            result.error = L.u3dg_last_error().decode()
+        return None, False
+    m = GaussianModel.zeros(n.value)
+    v = m.view()
+    check(L.u3dg_read_splat_ply(str(path).encode(), C.byref(v), n.value, C.byref(n), C.byref(is_splat)))
+    return m, bool(is_splat.value)
+
+
+def renderSh(model: GaussianModel, sh_rest: np.ndarray | None, degree: int, camera,
+             settings: RasterSettings | None = None) -> np.ndarray:
+    """Render with SH colours of degree 0..3 (ground-truth rendering of the synthetic scenes)."""
+    cs, ss = _cam(camera), _settings(settings)
+    rgb = np.zeros((cs.height, cs.width, 3), np.float32)
+    mv = model.view()
+    shp = _abi.fptr(np.ascontiguousarray(sh_rest, np.float32).reshape(-1)) if (sh_rest is not None and degree > 0) \
+        else None
+    check(load().u3dg_render_sh(C.byref(mv), shp, int(degree), C.byref(cs), C.byref(ss), _abi.fptr(rgb)))
+    return rgb
+
+
+def renderViewsSh(model: GaussianModel, sh_rest: np.ndarray | None, degree: int, cameras,
+                  settings: RasterSettings | None = None) -> list:
+    """Quantised (uint8) SH renders of many views with the model uploaded once: training targets."""
+    cams = (_abi.Camera * max(1, len(cameras)))()
+    sizes = []
+    for k, c in enumerate(cameras):
+        cams[k] = _cam(c)
+        sizes.append((cams[k].height, cams[k].width))
+    total = sum(h * w * 3 for h, w in sizes)
+    out = np.zeros(max(total, 1), np.uint8)
+    mv = model.view()
+    ss = _settings(settings)
+    shp = _abi.fptr(np.ascontiguousarray(sh_rest, np.float32).reshape(-1)) if (sh_rest is not None and degree > 0) \
+        else None
+    check(load().u3dg_render_views_sh(C.byref(mv), shp, int(degree), cams, len(cameras), C.byref(ss),
+                                      out.ctypes.data_as(_abi.u8p)))
+    res, o = [], 0
+    for h, w in sizes:
+        res.append(out[o:o + h * w * 3].reshape(h, w, 3).copy())
+        o += h * w * 3
+    return res
+
+
+__all__ = ["Trainer", "Rasterizer", "binTiles", "photometricLoss", "psnr", "Adam", "densifyAndPrune",
+           "initGaussiansFromPoints", "writeSplatPly", "readSplatPly", "renderSh", "U3dgError", "TrainImage"]

@@ -1,0 +1,345 @@
+// binning.cu - tile binning on the GPU (Rasterizer::binTiles, Rasterizer.cpp:206-261).
+//
+// The reference sorts the visible Gaussians by the float bits of their depth with a stable LSD
+// radix sort (ties keep index order), then buckets them per tile in that order, so every tile list
+// is depth-sorted. Here the same order comes from two stable radix sorts:
+//   1. (depth bits, Gaussian id) over all Gaussians -> depth rank; invisible ones get key
+//      0xFFFFFFFF and sort last;
+//   2. intersections are emitted in depth-rank order (an exclusive scan of per-rank tile counts
+//      gives each Gaussian its slots), keyed by tile id, and sorted stably by the tile id only.
+// Within a tile the emission order, i.e. (depth bits, id), survives, which is exactly the
+// reference's list. All sorts are stable 8-bit-digit LSD passes: per-block digit histograms, a
+// per-digit scan over blocks, and a scatter whose in-block ranks come from warp match-any votes.
+
+#include "kernels.h"
+
+namespace u3dg {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kItemsPerThread = 8;
+constexpr int kTile = kThreads * kItemsPerThread; // items per block
+constexpr int kWarps = kThreads / 32;
+constexpr int kRadix = 256;
+
+inline int numBlocks(int n) { return (n + kTile - 1) / kTile; }
+
+// Block-wide exclusive scan of one int per thread (blockDim == 256); returns the block total.
+__device__ __forceinline__ int blockExclusiveScan(int v, int &total)
+{
+    __shared__ int warpSums[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        warpSums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kWarps ? warpSums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o)
+                w += y;
+        }
+        if (lane < kWarps)
+            warpSums[lane] = w; // inclusive
+    }
+    __syncthreads();
+    total = warpSums[kWarps - 1];
+    const int before = warp > 0 ? warpSums[warp - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, int n, int shift, int *hist, int B)
+{
+    __shared__ int counts[kRadix];
+    counts[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kTile;
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        const int i = base + r * kThreads + threadIdx.x;
+        if (i < n)
+            atomicAdd(&counts[(keys[i] >> shift) & 0xFF], 1);
+    }
+    __syncthreads();
+    hist[threadIdx.x * B + blockIdx.x] = counts[threadIdx.x];
+}
+
+// One block per digit: exclusive scan of that digit's row of B block counts; rowTotals[d] = sum.
+__global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int B, int *rowTotals)
+{
+    int *row = hist + size_t(blockIdx.x) * B;
+    int carry = 0;
+    for (int c0 = 0; c0 < B; c0 += kThreads) {
+        const int i = c0 + threadIdx.x;
+        const int v = i < B ? row[i] : 0;
+        int total;
+        const int ex = blockExclusiveScan(v, total);
+        if (i < B)
+            row[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0)
+        rowTotals[blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
+                                                               uint32_t *keysOut, uint32_t *valsOut, int n, int shift,
+                                                               const int *hist, const int *rowTotals, int B)
+{
+    __shared__ int warpCounts[kWarps][kRadix];
+    __shared__ int base[kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < kWarps * kRadix; k += kThreads)
+        (&warpCounts[0][0])[k] = 0;
+    // Digit base: exclusive scan of the digit totals, plus this block's row prefix.
+    {
+        int total;
+        const int ex = blockExclusiveScan(rowTotals[threadIdx.x], total);
+        base[threadIdx.x] = ex + hist[threadIdx.x * B + blockIdx.x];
+    }
+    __syncthreads();
+    const uint32_t lanesBelow = (1u << lane) - 1u;
+    const int first = blockIdx.x * kTile + warp * (32 * kItemsPerThread);
+    uint32_t key[kItemsPerThread], val[kItemsPerThread];
+    int digit[kItemsPerThread], local[kItemsPerThread];
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        const int i = first + r * 32 + lane;
+        const bool valid = i < n;
+        key[r] = valid ? keysIn[i] : 0u;
+        val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
+        const int d = valid ? int((key[r] >> shift) & 0xFF) : kRadix;
+        digit[r] = d;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        int before = 0;
+        if (valid) {
+            before = warpCounts[warp][d];
+            local[r] = before + __popc(peers & lanesBelow);
+        }
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1)
+            warpCounts[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // Exclusive prefix of every digit over the warps (warps hold consecutive item ranges).
+    {
+        int s = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const int c = warpCounts[w][threadIdx.x];
+            warpCounts[w][threadIdx.x] = s;
+            s += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        const int d = digit[r];
+        if (d < kRadix) {
+            const int pos = base[d] + warpCounts[warp][d] + local[r];
+            keysOut[pos] = key[r];
+            valsOut[pos] = val[r];
+        }
+    }
+}
+
+// Exclusive scan, reduce-then-scan.
+__global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int n, int *partial)
+{
+    const int base = blockIdx.x * kTile;
+    int s = 0;
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        const int i = base + r * kThreads + threadIdx.x;
+        if (i < n)
+            s += in[i];
+    }
+    int total;
+    blockExclusiveScan(s, total);
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int B)
+{
+    int carry = 0;
+    for (int c0 = 0; c0 < B; c0 += kThreads) {
+        const int i = c0 + threadIdx.x;
+        const int v = i < B ? partial[i] : 0;
+        int total;
+        const int ex = blockExclusiveScan(v, total);
+        if (i < B)
+            partial[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0)
+        partial[B] = carry;
+}
+
+__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B)
+{
+    // Each thread owns kItemsPerThread consecutive items.
+    const int base = blockIdx.x * kTile + threadIdx.x * kItemsPerThread;
+    int v[kItemsPerThread];
+    int s = 0;
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        v[r] = (base + r < n) ? in[base + r] : 0;
+        s += v[r];
+    }
+    int total;
+    int run = blockExclusiveScan(s, total) + partial[blockIdx.x];
+#pragma unroll
+    for (int r = 0; r < kItemsPerThread; ++r) {
+        if (base + r < n)
+            out[base + r] = run;
+        run += v[r];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        out[n] = partial[B];
+}
+
+__global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt,
+                                 int *rankOf)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n)
+        return;
+    const int g = int(sortedIds[r]);
+    rankOf[g] = r;
+    int c = 0;
+    if (radius[g] > 0) {
+        const int4 q = rect[g];
+        c = (q.z - q.x) * (q.w - q.y);
+    }
+    cnt[r] = c;
+}
+
+// One thread per intersection: binary search of its rank in offs, then its tile in the rectangle
+// (row-major, as the reference's ty/tx loops).
+__global__ void emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
+                           uint32_t *keys, int *emitGid)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total)
+        return;
+    int lo = 0, hi = n; // last r with offs[r] <= e
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (offs[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const int g = int(sortedIds[lo]);
+    const int4 q = rect[g];
+    const int k = e - offs[lo];
+    const int w = q.z - q.x;
+    const int ty = q.y + k / w, tx = q.x + k % w;
+    keys[e] = uint32_t(ty * tilesX + tx);
+    emitGid[e] = g;
+}
+
+__global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, int total, int *list, int *inv)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < total) {
+        const int e = int(sortedEmit[s]);
+        list[s] = emitGid[e];
+        inv[e] = s;
+    }
+}
+
+__global__ void tileOffsetsKernel(const uint32_t *sortedKeys, int total, int tiles, int *tileOffsets)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > tiles)
+        return;
+    int lo = 0, hi = total; // first s with key >= t
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (int(sortedKeys[mid]) < t)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    tileOffsets[t] = (t == tiles) ? total : lo;
+}
+
+inline int grid(long long n, int t) { return int((n + t - 1) / t); }
+
+} // namespace
+
+size_t radixHistEntries(int n) { return size_t(kRadix) * size_t(numBlocks(n) > 0 ? numBlocks(n) : 1); }
+
+void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const uint32_t *valsIn, int n,
+                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s)
+{
+    uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
+    const uint32_t *vin = valsIn;
+    const int B = numBlocks(n);
+    if (n > 0) {
+        for (int shift = 0; shift < bits; shift += 8) {
+            { radixHistKernel<<<B, kThreads, 0, s>>>(kin, n, shift, hist, B); countLaunch(); }
+            { radixRowScanKernel<<<kRadix, kThreads, 0, s>>>(hist, B, rowTotals); countLaunch(); }
+            { radixScatterKernel<<<B, kThreads, 0, s>>>(kin, vin, kout, vout, n, shift, hist, rowTotals, B); countLaunch(); }
+            // The output of this pass is the input of the next one.
+            uint32_t *nk = kin;
+            kin = kout;
+            kout = nk;
+            vin = vout;
+            vout = (vout == valsB) ? valsA : valsB;
+        }
+    }
+    *keysOut = kin;
+    *valsOut = const_cast<uint32_t *>(vin);
+}
+
+size_t scanPartialEntries(int n) { return size_t(numBlocks(n)) + 1; }
+
+void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
+{
+    const int B = numBlocks(n);
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, sizeof(int), s);
+        return;
+    }
+    { scanReduceKernel<<<B, kThreads, 0, s>>>(in, n, partial); countLaunch(); }
+    { scanPartialKernel<<<1, kThreads, 0, s>>>(partial, B); countLaunch(); }
+    { scanDownsweepKernel<<<B, kThreads, 0, s>>>(in, out, n, partial, B); countLaunch(); }
+}
+
+void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt, int *rankOf,
+                      cudaStream_t s)
+{
+    if (n > 0)
+        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, n, cnt, rankOf); countLaunch(); }
+}
+
+void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
+                uint32_t *keys, int *emitGid, cudaStream_t s)
+{
+    if (total > 0)
+        { emitKernel<<<grid(total, 256), 256, 0, s>>>(sortedIds, offs, rect, n, total, tilesX, keys, emitGid); countLaunch(); }
+}
+
+void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, int total, int tiles,
+                        int *list, int *inv, int *tileOffsets, cudaStream_t s)
+{
+    if (total > 0)
+        { finalizeKernel<<<grid(total, 256), 256, 0, s>>>(sortedEmit, emitGid, total, list, inv); countLaunch(); }
+    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, total, tiles, tileOffsets); countLaunch(); }
+}
+
+} // namespace u3dg

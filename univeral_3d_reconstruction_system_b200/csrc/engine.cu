@@ -1,0 +1,445 @@
+// engine.cu - host orchestration of the GPU trainer: raster workspace, Trainer, densification.
+//
+// One CUDA stream per trainer. A step queues: projection, depth sort, per-rank tile counts + scan,
+// (one 4-byte read of the intersection count to size the intersection buffers), emission, tile
+// sort, tile offsets, compositing forward, loss forward/backward + stats, compositing backward, and
+// the chain rule fused with Adam. The training RNG (std::mt19937, Trainer.h:79) stays on the host so
+// the view order and the split samples are the reference's exactly.
+
+#include "engine.h"
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+namespace u3dg {
+
+static std::atomic<unsigned long long> gLaunches{0};
+
+void countLaunch() { gLaunches.fetch_add(1, std::memory_order_relaxed); }
+
+unsigned long long launchCount() { return gLaunches.load(std::memory_order_relaxed); }
+
+void checkSettings(const u3dg_raster_settings &st)
+{
+    if (!(st.tile_size == 8 || (st.tile_size >= 16 && st.tile_size % 16 == 0 && st.tile_size <= 256)))
+        throw StatusError(U3DG_ERR_INVALID_ARG,
+                          "tile_size must be 8 or a multiple of 16 up to 256, got " + std::to_string(st.tile_size));
+}
+
+void checkCamera(const u3dg_camera &cam)
+{
+    if (cam.width <= 0 || cam.height <= 0 || cam.width > 16384 || cam.height > 16384)
+        throw StatusError(U3DG_ERR_INVALID_ARG, "camera size must be 1..16384 pixels per side");
+    if (!(cam.fx != 0.0f) || !(cam.fy != 0.0f))
+        throw StatusError(U3DG_ERR_INVALID_ARG, "camera focal lengths must be non-zero");
+}
+
+// ------------------------------------------------------------------ raster workspace
+
+void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
+                              const float *shRest, int shDegree, cudaStream_t stream)
+{
+    checkSettings(s);
+    checkCamera(c);
+    cam = c;
+    st = s;
+    n = count;
+    tilesX = (cam.width + st.tile_size - 1) / st.tile_size;
+    tilesY = (cam.height + st.tile_size - 1) / st.tile_size;
+    const size_t nn = size_t(std::max(n, 1));
+    rec.reserve(nn);
+    depthKey.reserve(nn);
+    sortKeys.reserve(nn);
+    sortVals0.reserve(nn);
+    sortVals1.reserve(nn);
+    depth.reserve(nn);
+    rect.reserve(nn);
+    radius.reserve(nn);
+    rankOf.reserve(nn);
+    cnt.reserve(nn);
+    offs.reserve(nn + 1);
+    scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
+    flags.reserve(nn);
+    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p};
+    launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream);
+}
+
+void RasterWorkspace::bin(cudaStream_t stream)
+{
+    const int tiles = tilesX * tilesY;
+    hist.reserve(std::max(radixHistEntries(n), size_t(256)));
+    rowTotals.reserve(256);
+    uint32_t *keysOut = nullptr, *valsOut = nullptr;
+    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, nullptr, n, 32, hist.p, rowTotals.p, &keysOut,
+                   &valsOut, stream);
+    sortedIds = valsOut;
+    launchRankCounts(sortedIds, rect.p, radius.p, n, cnt.p, rankOf.p, stream);
+    exclusiveScan(cnt.p, offs.p, n, scanPartial.p, stream);
+    hostTotal.reserve(1);
+    U3DG_CUDA(cudaMemcpyAsync(hostTotal.p, offs.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    U3DG_CUDA(cudaStreamSynchronize(stream));
+    total = *hostTotal.p;
+    if (total < 0)
+        throw StatusError(U3DG_ERR_CAPACITY, "tile-Gaussian intersection count overflowed 32 bits");
+    const size_t tt = size_t(std::max(total, 1));
+    iKeys0.reserve(tt);
+    iKeys1.reserve(tt);
+    iVals0.reserve(tt);
+    iVals1.reserve(tt);
+    emitGid.reserve(tt);
+    list.reserve(tt);
+    inv.reserve(tt);
+    partial.reserve(tt * kG2d);
+    hist.reserve(std::max(radixHistEntries(total), size_t(256)));
+    tileOffsets.reserve(size_t(tiles) + 1);
+    launchEmit(sortedIds, offs.p, rect.p, n, total, tilesX, iKeys0.p, emitGid.p, stream);
+    int bits = 0;
+    while ((1 << bits) < tiles)
+        ++bits;
+    bits = std::max(bits, 1);
+    radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, nullptr, total, bits, hist.p, rowTotals.p, &keysOut,
+                   &valsOut, stream);
+    launchFinalizeBins(keysOut, valsOut, emitGid.p, total, tiles, list.p, inv.p, tileOffsets.p, stream);
+}
+
+RasterArgs RasterWorkspace::rasterArgs() const
+{
+    RasterArgs a;
+    a.tileOffsets = tileOffsets.p;
+    a.list = list.p;
+    a.rec = rec.p;
+    a.width = cam.width;
+    a.height = cam.height;
+    a.tileSize = st.tile_size;
+    a.tilesX = tilesX;
+    for (int k = 0; k < 3; ++k)
+        a.bg[k] = st.background[k];
+    a.minAlpha = st.min_alpha;
+    a.minTransmittance = st.min_transmittance;
+    return a;
+}
+
+void RasterWorkspace::composite(cudaStream_t stream)
+{
+    const size_t P = size_t(cam.width) * cam.height;
+    rgb.reserve(P * 3);
+    finalT.reserve(P);
+    nContrib.reserve(P);
+    launchCompositeForward(rasterArgs(), rgb.p, finalT.p, nContrib.p, stream);
+}
+
+void RasterWorkspace::backwardComposite(const float *dLdRgb, cudaStream_t stream)
+{
+    if (st.tile_size > 16 && total > 0)
+        U3DG_CUDA(cudaMemsetAsync(partial.p, 0, size_t(total) * kG2d * sizeof(float), stream));
+    launchCompositeBackward(rasterArgs(), dLdRgb, finalT.p, nContrib.p, partial.p, stream);
+}
+
+ChainArgs RasterWorkspace::chainArgs(const Params &P) const
+{
+    ChainArgs a{};
+    a.params = P;
+    a.n = n;
+    a.cam = cam;
+    a.st = st;
+    a.radius = radius.p;
+    a.rec = rec.p;
+    a.flags = flags.p;
+    a.rankOf = rankOf.p;
+    a.offs = offs.p;
+    a.inv = inv.p;
+    a.partial = partial.p;
+    return a;
+}
+
+// ------------------------------------------------------------------ trainer
+
+void copyModelToArena(float *base, size_t cap, const u3dg_model &m, cudaStream_t s)
+{
+    const Params P = paramsAt(base, cap);
+    const size_t n = m.count;
+    if (n == 0)
+        return;
+    U3DG_CUDA(cudaMemcpyAsync(P.means, m.means, n * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+    U3DG_CUDA(cudaMemcpyAsync(P.scales, m.scales, n * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+    U3DG_CUDA(cudaMemcpyAsync(P.quats, m.quats, n * 4 * sizeof(float), cudaMemcpyHostToDevice, s));
+    U3DG_CUDA(cudaMemcpyAsync(P.opac, m.opacities, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    U3DG_CUDA(cudaMemcpyAsync(P.colors, m.colors, n * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+}
+
+static void copyArenaToModel(const float *base, size_t cap, size_t n, u3dg_model &m, cudaStream_t s)
+{
+    const Params P = paramsAt(const_cast<float *>(base), cap);
+    if (n == 0)
+        return;
+    U3DG_CUDA(cudaMemcpyAsync(m.means, P.means, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(m.scales, P.scales, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(m.quats, P.quats, n * 4 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(m.opacities, P.opac, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(m.colors, P.colors, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+}
+
+TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int count, float sceneExtent,
+                         const u3dg_train_options &opt)
+    : o(opt), rng(opt.seed)
+{
+    checkSettings(o.raster);
+    if (count < 0 || (count > 0 && imgs == nullptr))
+        throw StatusError(U3DG_ERR_INVALID_ARG, "image list is invalid");
+    if (initial.count > 0 && (!initial.means || !initial.scales || !initial.quats || !initial.opacities || !initial.colors))
+        throw StatusError(U3DG_ERR_INVALID_ARG, "initial model has null arrays");
+    if (initial.count > size_t(INT_MAX / 64))
+        throw StatusError(U3DG_ERR_CAPACITY, "too many Gaussians");
+    if (o.refine_interval <= 0)
+        throw StatusError(U3DG_ERR_INVALID_ARG, "refine_interval must be positive");
+    U3DG_CUDA(cudaGetDevice(&device));
+    U3DG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    extent = std::max(sceneExtent, 1e-6f);
+    n = int(initial.count);
+    cap = std::max<size_t>(size_t(std::max(o.max_gaussians, 0)), initial.count);
+    cap = std::max<size_t>(cap, 1);
+    for (auto &a : arena)
+        a.reserve(42 * cap, true);
+    U3DG_CUDA(cudaMemsetAsync(arena[cur].p, 0, 42 * cap * sizeof(float), stream));
+    copyModelToArena(arena[cur].p, cap, initial, stream);
+    gradAccum.reserve(cap, true);
+    gradCount.reserve(cap, true);
+    U3DG_CUDA(cudaMemsetAsync(gradAccum.p, 0, cap * sizeof(float), stream));
+    U3DG_CUDA(cudaMemsetAsync(gradCount.p, 0, cap * sizeof(int), stream));
+    size_t total = 0, maxP = 1;
+    for (int k = 0; k < count; ++k) {
+        checkCamera(imgs[k].camera);
+        if (!imgs[k].rgb)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "image " + std::to_string(k) + " has no pixels");
+        cams.push_back(imgs[k].camera);
+        imageOffset.push_back(total);
+        const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
+        total += P * 3;
+        maxP = std::max(maxP, P);
+    }
+    images.reserve(std::max<size_t>(total, 1), true);
+    for (int k = 0; k < count; ++k) {
+        const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
+        U3DG_CUDA(cudaMemcpyAsync(images.p + imageOffset[size_t(k)], imgs[k].rgb, P * 3, cudaMemcpyHostToDevice, stream));
+    }
+    dLoss.reserve(maxP * 3);
+    abc.reserve(maxP * 9);
+    dStats.reserve(1, true);
+    hStats.reserve(1);
+    U3DG_CUDA(cudaMemsetAsync(dStats.p, 0, sizeof(DevStats), stream));
+    std::memset(hStats.p, 0, sizeof(DevStats));
+    hCounts.reserve(4);
+    // The host buffers of the caller may be released after this call returns.
+    U3DG_CUDA(cudaStreamSynchronize(stream));
+}
+
+TrainerImpl::~TrainerImpl()
+{
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    delete timer;
+}
+
+void TrainerImpl::sync() { U3DG_CUDA(cudaStreamSynchronize(stream)); }
+
+void TrainerImpl::step()
+{
+    if (cams.empty() || done())
+        return;
+    // View order: one shuffle of all views per epoch (Trainer.cpp:57-64).
+    if (orderPos >= order.size()) {
+        order.resize(cams.size());
+        for (size_t k = 0; k < order.size(); ++k)
+            order[k] = int(k);
+        std::shuffle(order.begin(), order.end(), rng);
+        orderPos = 0;
+    }
+    const size_t v = size_t(order[orderPos++]);
+    const u3dg_camera &cam = cams[v];
+    const uint8_t *target = images.p + imageOffset[v];
+    const int W = cam.width, H = cam.height;
+    PhaseTimer *tm = profiling ? timer : nullptr;
+    if (tm)
+        tm->mark(0, stream);
+    ws.project(params(), n, cam, o.raster, nullptr, 0, stream);
+    if (tm)
+        tm->mark(1, stream);
+    ws.bin(stream);
+    if (tm)
+        tm->mark(2, stream);
+    ws.composite(stream);
+    if (tm)
+        tm->mark(3, stream);
+    // Loss (Trainer.cpp:67-71) and the step's stats (Trainer.cpp:88-92).
+    const int lb = lossBlocks(W, H);
+    lossBlockSums.reserve(size_t(lb) * 3);
+    LossScratch ls{abc.p, lossBlockSums.p, lb};
+    launchLoss(ws.rgb.p, nullptr, target, W, H, o.ssim_lambda, dLoss.p, ls, stream);
+    launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, iteration + 1, nullptr, nullptr, stream);
+    if (tm)
+        tm->mark(4, stream);
+    ws.backwardComposite(dLoss.p, stream);
+    if (tm)
+        tm->mark(5, stream);
+    // Means learning rate decays exponentially and scales with the scene (Trainer.cpp:81-85);
+    // Adam bias corrections as Adam::step (Adam.cpp:68-71), all in host float like the reference.
+    const float t = float(iteration) / float(std::max(1, o.iterations - 1));
+    const float lrMeans = std::exp(std::log(o.lr.means) * (1 - t) + std::log(o.means_lr_final) * t) * extent;
+    ++adamStep;
+    const float bc1 = 1.0f - std::pow(0.9f, float(adamStep));
+    const float bc2 = 1.0f - std::pow(0.999f, float(adamStep));
+    ChainArgs a = ws.chainArgs(params());
+    a.gradAccum = gradAccum.p;
+    a.gradCount = gradCount.p;
+    a.m = moment1();
+    a.v = moment2();
+    const float lrs[5] = {lrMeans, o.lr.scales, o.lr.quats, o.lr.opacities, o.lr.colors};
+    for (int k = 0; k < 5; ++k)
+        a.stepSize[k] = lrs[k] / bc1;
+    a.invSqrtBc2 = 1.0f / std::sqrt(bc2);
+    launchChain(a, true, stream);
+    U3DG_CUDA(cudaGetLastError());
+    if (tm)
+        tm->mark(6, stream);
+    ++iteration;
+    if (iteration >= o.refine_start && iteration < o.refine_stop && iteration % o.refine_interval == 0)
+        densifyAndPrune();
+    if (o.opacity_reset_interval > 0 && iteration < o.refine_stop && iteration % o.opacity_reset_interval == 0)
+        resetOpacity();
+    U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
+    if (tm) {
+        tm->mark(7, stream);
+        U3DG_CUDA(cudaEventSynchronize(tm->ev[7]));
+        u3dg_phase_times &acc = tm->acc;
+        acc.steps += 1;
+        acc.project_ms += tm->between(0, 1);
+        acc.sort_ms += tm->between(1, 2);
+        acc.forward_ms += tm->between(2, 3);
+        acc.loss_ms += tm->between(3, 4);
+        acc.backward_ms += tm->between(4, 5);
+        acc.update_ms += tm->between(5, 6);
+        acc.densify_ms += tm->between(6, 7);
+        acc.total_ms += tm->between(0, 7);
+        acc.intersections += uint64_t(ws.total);
+        acc.gaussians += uint64_t(ws.n);
+        acc.pixels += uint64_t(W) * uint64_t(H);
+    }
+}
+
+DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng)
+{
+    cudaStream_t s = t.stream;
+    const int n = t.n;
+    const u3dg_train_options &o = t.o;
+    DensifyResult r{n, 0, 0, 0};
+    if (n <= 0)
+        return r;
+    const size_t nn = size_t(n) + 1;
+    for (DevBuf<int> *b : {&t.keep, &t.cost, &t.costScan, &t.accCost, &t.accScan, &t.isSplit, &t.splitScan, &t.keepScan})
+        b->reserve(nn);
+    t.firstSecond.reserve(2);
+    t.dScanPartial.reserve(scanPartialEntries(n) + 1);
+    const float splitScale = o.percent_dense * t.extent;
+    const long long budget = o.max_gaussians > n ? (long long)o.max_gaussians - n : 0;
+    const Params P = t.params();
+    launchDensifyClassify(P, n, t.gradAccum.p, t.gradCount.p, t.extent, splitScale, o.prune_opacity,
+                          o.densify_grad_threshold, t.opacityWasReset ? 1 : 0, t.keep.p, t.cost.p, s);
+    exclusiveScan(t.cost.p, t.costScan.p, n, t.dScanPartial.p, s);
+    U3DG_CUDA(cudaMemsetAsync(t.firstSecond.p, 0x7F, 2 * sizeof(int), s)); // 0x7F7F7F7F: "none" (>= n)
+    launchDensifySelect(n, t.cost.p, t.costScan.p, budget, t.firstSecond.p, t.keep.p, t.accCost.p, t.isSplit.p, s);
+    exclusiveScan(t.keep.p, t.keepScan.p, n, t.dScanPartial.p, s);
+    exclusiveScan(t.accCost.p, t.accScan.p, n, t.dScanPartial.p, s);
+    exclusiveScan(t.isSplit.p, t.splitScan.p, n, t.dScanPartial.p, s);
+    t.hCounts.reserve(4);
+    U3DG_CUDA(cudaMemcpyAsync(t.hCounts.p + 0, t.keepScan.p + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(t.hCounts.p + 1, t.accScan.p + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaMemcpyAsync(t.hCounts.p + 2, t.splitScan.p + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    U3DG_CUDA(cudaStreamSynchronize(s));
+    const int kept = t.hCounts.p[0], added = t.hCounts.p[1], splits = t.hCounts.p[2];
+    // Split samples: 6 per accepted split, in index order, c = 0..1, k = 0..2 (Trainer.cpp:114,145-150).
+    // A fresh distribution per call, as the reference constructs one per densifyAndPrune.
+    std::normal_distribution<float> normal(0.0f, 1.0f);
+    const size_t ns = size_t(splits) * 6;
+    t.hNormals.reserve(std::max<size_t>(ns, 1));
+    for (size_t k = 0; k < ns; ++k)
+        t.hNormals.p[k] = normal(rng);
+    t.normals.reserve(std::max<size_t>(ns, 1));
+    if (ns > 0)
+        U3DG_CUDA(cudaMemcpyAsync(t.normals.p, t.hNormals.p, ns * sizeof(float), cudaMemcpyHostToDevice, s));
+    const int other = 1 - t.cur;
+    launchDensifyWrite(P, t.moment1(), t.moment2(), t.paramsOf(other, 0), t.paramsOf(other, 1), t.paramsOf(other, 2), n,
+                       t.keep.p, t.keepScan.p, t.accCost.p, t.accScan.p, t.isSplit.p, t.splitScan.p, kept, t.normals.p,
+                       std::log(1.6f), s);
+    U3DG_CUDA(cudaGetLastError());
+    t.cur = other;
+    r.newCount = kept + added;
+    r.splits = splits;
+    r.clones = added - 2 * splits;
+    r.pruned = n - kept - splits;
+    t.n = r.newCount;
+    U3DG_CUDA(cudaMemsetAsync(t.gradAccum.p, 0, size_t(t.n) * sizeof(float), s));
+    U3DG_CUDA(cudaMemsetAsync(t.gradCount.p, 0, size_t(t.n) * sizeof(int), s));
+    // hNormals is read by the copy above; keep it valid until the copy is done.
+    U3DG_CUDA(cudaStreamSynchronize(s));
+    return r;
+}
+
+void TrainerImpl::densifyAndPrune()
+{
+    const DensifyResult r = densifyOnDevice(*this, rng);
+    lastPruned = r.pruned;
+    lastClones = r.clones;
+    lastSplits = r.splits;
+}
+
+void TrainerImpl::resetOpacity()
+{
+    // logit(0.01f) in host float arithmetic (GaussianModel.h:13, Trainer.cpp:173).
+    const float cap01 = std::log(0.01f / (1.0f - 0.01f));
+    launchOpacityReset(params().opac, moment1().opac, moment2().opac, n, cap01, stream);
+    opacityWasReset = true;
+}
+
+float TrainerImpl::evaluatePsnr()
+{
+    if (cams.empty())
+        return 0.0f;
+    constexpr int kSq = 297; // sqDiff partial blocks + 1 (loss.cu)
+    psnrSums.reserve(cams.size() * kSq);
+    for (size_t v = 0; v < cams.size(); ++v) {
+        ws.forward(params(), n, cams[v], o.raster, nullptr, 0, stream);
+        const size_t count = size_t(cams[v].width) * cams[v].height * 3;
+        launchPsnrU8(ws.rgb.p, images.p + imageOffset[v], count, psnrSums.p + v * kSq, stream);
+    }
+    std::vector<double> sums(cams.size() * kSq);
+    U3DG_CUDA(cudaMemcpyAsync(sums.data(), psnrSums.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    sync();
+    double total = 0;
+    for (size_t v = 0; v < cams.size(); ++v) {
+        const size_t count = size_t(cams[v].width) * cams[v].height * 3;
+        const double mse = sums[v * kSq + kSq - 1] / double(std::max<size_t>(count, 1));
+        total += mse <= 1e-12 ? 99.0f : float(-10.0 * std::log10(mse)); // psnr, Loss.cpp:187-196
+    }
+    return float(total / double(cams.size()));
+}
+
+void TrainerImpl::render(const u3dg_camera &c, float *hostRgb)
+{
+    ws.forward(params(), n, c, o.raster, nullptr, 0, stream);
+    U3DG_CUDA(cudaMemcpyAsync(hostRgb, ws.rgb.p, size_t(c.width) * c.height * 3 * sizeof(float), cudaMemcpyDeviceToHost,
+                              stream));
+    sync();
+}
+
+void TrainerImpl::download(u3dg_model &out)
+{
+    copyArenaToModel(arena[cur].p, cap, size_t(n), out, stream);
+    sync();
+}
+
+} // namespace u3dg

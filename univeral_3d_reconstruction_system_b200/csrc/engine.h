@@ -1,0 +1,229 @@
+// engine.h - host-side objects behind the C ABI: device buffers, the raster workspace and the trainer.
+#pragma once
+
+#include "kernels.h"
+
+#include <cstdio>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace u3dg {
+
+// A failed CUDA call, carried to the C ABI boundary and turned into a status code there.
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char *expr, const char *file, int line)
+        : std::runtime_error(std::string(expr) + ": " + cudaGetErrorString(c) + " (" + file + ":" + std::to_string(line) + ")"),
+          code(c)
+    {
+    }
+};
+
+struct StatusError : std::runtime_error {
+    int status;
+    StatusError(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+#define U3DG_CUDA(x)                                                   \
+    do {                                                               \
+        cudaError_t e_ = (x);                                          \
+        if (e_ != cudaSuccess)                                         \
+            throw ::u3dg::CudaError(e_, #x, __FILE__, __LINE__);       \
+    } while (0)
+
+// Device array with capacity growth (cudaMalloc only when it has to grow).
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    // Ensures room for n elements; contents are NOT preserved when it grows.
+    void reserve(size_t n, bool exact = false)
+    {
+        if (n <= cap && p)
+            return;
+        release();
+        size_t c = exact ? n : std::max(n, cap + cap / 2);
+        if (c == 0)
+            c = 1;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&p), c * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            throw StatusError(U3DG_ERR_OOM, "cudaMalloc of " + std::to_string(c * sizeof(T)) + " bytes failed: " +
+                                                cudaGetErrorString(e));
+        }
+        cap = c;
+    }
+};
+
+// Pinned host array (for asynchronous device->host reads).
+template <class T>
+struct HostPinned {
+    T *p = nullptr;
+    size_t cap = 0;
+    ~HostPinned()
+    {
+        if (p)
+            cudaFreeHost(p);
+    }
+    void reserve(size_t n)
+    {
+        if (n <= cap && p)
+            return;
+        if (p)
+            cudaFreeHost(p);
+        p = nullptr;
+        U3DG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&p), std::max<size_t>(n, 1) * sizeof(T)));
+        cap = std::max<size_t>(n, 1);
+    }
+};
+
+unsigned long long launchCount();
+void checkSettings(const u3dg_raster_settings &st);
+// Uploads a host model into the params slot of an arena of capacity `cap`.
+void copyModelToArena(float *base, size_t cap, const u3dg_model &m, cudaStream_t s);
+void checkCamera(const u3dg_camera &cam);
+
+// Everything Rasterizer::forward keeps between forward and backward (Rasterizer.h:57-89), on the GPU.
+struct RasterWorkspace {
+    // per Gaussian
+    DevBuf<SplatRec> rec;
+    DevBuf<uint32_t> depthKey, sortKeys, sortVals0, sortVals1;
+    DevBuf<float> depth;
+    DevBuf<int4> rect;
+    DevBuf<int> radius, rankOf, cnt, offs, scanPartial, hist, rowTotals;
+    DevBuf<uint8_t> flags;
+    // per intersection
+    DevBuf<uint32_t> iKeys0, iKeys1, iVals0, iVals1;
+    DevBuf<int> emitGid, list, inv;
+    DevBuf<float> partial;
+    // per tile / pixel
+    DevBuf<int> tileOffsets, nContrib;
+    DevBuf<float> rgb, finalT;
+    HostPinned<int> hostTotal;
+
+    int n = 0, total = 0, tilesX = 0, tilesY = 0;
+    u3dg_camera cam{};
+    u3dg_raster_settings st{};
+    uint32_t *sortedIds = nullptr;
+    // Device-side event of the last binning readback (for profiling).
+    void project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
+                 int shDegree, cudaStream_t stream);
+    // Depth sort + tile binning from depthKey / rect / radius (waits for the intersection count).
+    void bin(cudaStream_t stream);
+    void composite(cudaStream_t stream);
+    void forward(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
+                 int shDegree, cudaStream_t stream)
+    {
+        project(P, count, c, s, shRest, shDegree, stream);
+        bin(stream);
+        composite(stream);
+    }
+    // Compositing backward into `partial`.
+    void backwardComposite(const float *dLdRgb, cudaStream_t stream);
+    RasterArgs rasterArgs() const;
+    ChainArgs chainArgs(const Params &P) const;
+};
+
+// CUDA events around the phases of a profiled step.
+struct PhaseTimer {
+    static constexpr int kEvents = 8;
+    cudaEvent_t ev[kEvents];
+    u3dg_phase_times acc{};
+    PhaseTimer()
+    {
+        for (auto &e : ev)
+            U3DG_CUDA(cudaEventCreate(&e));
+    }
+    ~PhaseTimer()
+    {
+        for (auto &e : ev)
+            cudaEventDestroy(e);
+    }
+    void mark(int k, cudaStream_t s) { U3DG_CUDA(cudaEventRecord(ev[k], s)); }
+    float between(int a, int b)
+    {
+        float ms = 0;
+        U3DG_CUDA(cudaEventElapsedTime(&ms, ev[a], ev[b]));
+        return ms;
+    }
+};
+
+
+// The GPU Trainer (Trainer.h:47-93, Trainer.cpp).
+struct TrainerImpl {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    u3dg_train_options o{};
+    float extent = 1.0f;
+    size_t cap = 0;
+    int n = 0;
+    int cur = 0;                      // which arena holds the live model
+    DevBuf<float> arena[2];           // params, m, v: 3 * 14 * cap floats each
+    DevBuf<float> gradAccum;
+    DevBuf<int> gradCount;
+    std::vector<u3dg_camera> cams;
+    std::vector<size_t> imageOffset;
+    DevBuf<uint8_t> images;
+    RasterWorkspace ws;
+    DevBuf<float> dLoss, abc;
+    DevBuf<double> lossBlockSums, psnrSums;
+    DevBuf<DevStats> dStats;
+    HostPinned<DevStats> hStats;
+    // densification scratch
+    DevBuf<int> keep, cost, costScan, accCost, accScan, isSplit, splitScan, keepScan, firstSecond, dScanPartial;
+    DevBuf<float> normals;
+    HostPinned<int> hCounts;
+    HostPinned<float> hNormals;
+
+    std::mt19937 rng;
+    std::vector<int> order;
+    size_t orderPos = 0;
+    int iteration = 0;
+    int adamStep = 0;
+    bool opacityWasReset = false;
+    int lastPruned = 0, lastClones = 0, lastSplits = 0;
+
+    bool profiling = false;
+    PhaseTimer *timer = nullptr;
+
+    TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int count, float sceneExtent,
+                const u3dg_train_options &opt);
+    ~TrainerImpl();
+
+    Params params() { return paramsAt(arena[cur].p, cap); }
+    Params moment1() { return paramsAt(arena[cur].p + 14 * cap, cap); }
+    Params moment2() { return paramsAt(arena[cur].p + 28 * cap, cap); }
+    Params paramsOf(int which, int k) { return paramsAt(arena[which].p + size_t(k) * 14 * cap, cap); }
+
+    bool done() const { return iteration >= o.iterations; }
+    void step();
+    void densifyAndPrune();
+    void resetOpacity();
+    float evaluatePsnr();
+    void render(const u3dg_camera &c, float *hostRgb);
+    void download(u3dg_model &out);
+    void sync();
+};
+
+// Densification on device arrays (shared by the trainer and the unit entry point).
+struct DensifyResult {
+    int newCount;
+    int pruned, clones, splits;
+};
+DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng);
+
+} // namespace u3dg

@@ -1,0 +1,111 @@
+// kernels.h - host-side launch interface of the CUDA kernels (no torch, plain pointers).
+#pragma once
+
+#include "common.cuh"
+
+namespace u3dg {
+
+// Outputs of the projection kernel, one entry per Gaussian.
+struct ProjOut {
+    SplatRec *rec;      // raster record (valid where radius > 0)
+    uint32_t *depthKey; // float bits of the camera-space depth; 0xFFFFFFFF when not visible
+    float *depth;       // camera-space depth (valid where radius > 0)
+    int4 *rect;         // tile rectangle x0, y0, x1, y1 (exclusive)
+    int *radius;        // 0 = not visible
+    uint8_t *flags;     // bit0/1: J clamped in x/y; bit2..4: colour clamped
+};
+
+// Arguments of the chain-rule kernel (backward pass 2), optionally fused with Adam.
+struct ChainArgs {
+    Params params;
+    int n;
+    u3dg_camera cam;
+    u3dg_raster_settings st;
+    const int *radius;
+    const SplatRec *rec;
+    const uint8_t *flags;
+    const int *rankOf;    // depth rank of every Gaussian
+    const int *offs;      // per rank: first intersection in emission order (n + 1 entries)
+    const int *inv;       // emission index -> tile-sorted index
+    const float *partial; // per tile-sorted intersection: 9 summed 2D gradients
+    float *gradAccum;     // |dL/dmean2d| NDC statistic (may be null)
+    int *gradCount;       // visibility count (may be null)
+    Params grads;         // non-Adam mode: gradients are added here
+    Params m, v;          // Adam mode: moments
+    float stepSize[5];    // Adam mode: lr / bc1 per group
+    float invSqrtBc2;
+};
+
+// gaussian.cu
+void launchProject(const Params &P, int n, const u3dg_camera &cam, const u3dg_raster_settings &st, int tilesX,
+                   int tilesY, const float *shRest, int shDegree, const ProjOut &out, cudaStream_t s);
+void launchChain(const ChainArgs &a, bool adam, cudaStream_t s);
+void launchAdamSegment(float *p, const float *g, float *m, float *v, int len, float stepSize, float invSqrtBc2,
+                       cudaStream_t s);
+void launchDensifyClassify(const Params &P, int n, const float *gradAccum, const int *gradCount, float extent,
+                           float splitScale, float pruneOpacity, float gradThreshold, int opacityWasReset, int *keep,
+                           int *cost, cudaStream_t s);
+void launchDensifySelect(int n, const int *cost, const int *costScan, long long budget, int *firstSecond, int *keep,
+                         int *accCost, int *isSplit, cudaStream_t s);
+void launchDensifyWrite(const Params &P, const Params &M, const Params &V, const Params &P2, const Params &M2,
+                        const Params &V2, int n, const int *keep, const int *keepScan, const int *accCost,
+                        const int *accScan, const int *isSplit, const int *splitScan, int keptTotal,
+                        const float *normals, float log16, cudaStream_t s);
+void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float cap, cudaStream_t s);
+
+// binning.cu
+// Scratch needed by radixSortPairs for n items: two key and two value buffers of n entries plus
+// the histogram of radixHistEntries(n) ints.
+size_t radixHistEntries(int n);
+// Stable LSD radix sort of (key, value) pairs on key bits [0, bits); values == nullptr means the
+// initial values are the item indices. Result in *keysOut / *valsOut (one of the two buffers).
+void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const uint32_t *valsIn, int n,
+                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s);
+// Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
+size_t scanPartialEntries(int n);
+void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
+// Per depth rank: tile count of the Gaussian and the inverse map gid -> rank.
+void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt, int *rankOf,
+                      cudaStream_t s);
+// Emission of the intersections in depth-rank order: tile key and Gaussian id per intersection.
+void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
+                uint32_t *keys, int *emitGid, cudaStream_t s);
+// After the tile sort: Gaussian id per sorted entry, inverse permutation, tile offsets.
+void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, int total, int tiles,
+                        int *list, int *inv, int *tileOffsets, cudaStream_t s);
+
+// raster.cu
+struct RasterArgs {
+    const int *tileOffsets;
+    const int *list;
+    const SplatRec *rec;
+    int width, height, tileSize, tilesX;
+    float bg[3];
+    float minAlpha, minTransmittance;
+};
+void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s);
+// partial: 9 floats per tile-sorted entry; zeroed by the caller when tileSize > 16 (atomics).
+void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
+                             float *partial, cudaStream_t s);
+
+// loss.cu
+struct LossScratch {
+    float *abc;        // 3 maps x 3 channels x P
+    double *blockSums; // 3 doubles per block: l1, ssim, squared error
+    int blocks;
+};
+int lossBlocks(int width, int height);
+// target is either float (targetF) or uint8 (targetU8, converted as float(u8) * (1/255f)).
+void launchLoss(const float *render, const float *targetF, const uint8_t *targetU8, int width, int height, float lambda,
+                float *grad, const LossScratch &ls, cudaStream_t s);
+// Reduces the block sums into the step's LossValue / PSNR and updates the EMA stats
+// (Trainer.cpp:88-92). out3 (may be null) gets total, l1, ssim; psnrOut (may be null) the PSNR.
+void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
+                        float *out3, float *psnrOut, cudaStream_t s);
+// PSNR of the render against a uint8 target, accumulated in double (evaluatePsnr).
+void launchPsnrU8(const float *render, const uint8_t *target, size_t count, double *sumOut, cudaStream_t s);
+void launchPsnrF(const float *a, const float *b, size_t count, double *sumOut, cudaStream_t s);
+// TrainImage::quantize on the device: lround(clamp(v, 0, 1) * 255) per value.
+void launchQuantize(const float *rgb, size_t count, uint8_t *out, cudaStream_t s);
+
+} // namespace u3dg
