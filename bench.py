@@ -132,13 +132,22 @@ class ClockSampler:
 # ------------------------------------------------------------------ workload
 
 
-def build_workload(render_on_gpu: bool, seed: int = 0):
-    """The High scene, its ground-truth images and the 300k-Gaussian initial model."""
+WORKLOADS = {
+    # name: (scene preset, model Gaussians)
+    "high-300k": ("high", 300_000),
+    "balanced-150k": ("balanced", 150_000),
+    "fast-80k": ("fast", 80_000),
+}
+
+
+def build_workload(render_on_gpu: bool, seed: int = 0, workload: str = "high-300k"):
+    """The preset scene, its ground-truth images and an initial model at the preset's Gaussian cap."""
     from univeral_3d_reconstruction_system_b200.scenes import dense_init_points, make_scene
     from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
 
     t0 = time.time()
-    sc = make_scene("high", seed)
+    preset, cap = WORKLOADS[workload]
+    sc = make_scene(preset, seed)
     st = RasterSettings()
     if render_on_gpu:
         from univeral_3d_reconstruction_system_b200 import api
@@ -148,7 +157,7 @@ def build_workload(render_on_gpu: bool, seed: int = 0):
         orc = Oracle()
         imgs = [TrainImage.quantize(orc.render(sc.truth, c, st, sc.sh_rest, 3)) for c in sc.cameras]
     sc.images = [TrainImage(c, im) for c, im in zip(sc.cameras, imgs)]
-    xyz, rgb = dense_init_points(sc, MODEL_CAP)
+    xyz, rgb = dense_init_points(sc, cap)
     opt = sc.options()  # TrainOptions::forIterations(7000), max 300k
     opt.refine_start = opt.iterations + 1  # steady phase: no densification, no opacity reset
     opt.opacity_reset_interval = 0
@@ -177,9 +186,21 @@ def run_ours(args, dist: Dist) -> dict:
 
     L = _lib.load()
     _lib.check(L.u3dg_set_device(dist.local))
-    sc, xyz, rgb, opt = build_workload(render_on_gpu=True, seed=0)
+    sc, xyz, rgb, opt = build_workload(render_on_gpu=True, seed=0, workload=args.workload)
+    args.built = (sc, xyz, rgb, opt)
     init = api.initGaussiansFromPoints(xyz, rgb)
     W, K = args.warmup, args.steps
+    if args.ncu_steps:
+        # Profiling run: warm up, report how many kernels ran before the captured steps, run them.
+        opt.iterations = max(opt.iterations, W + args.ncu_steps + 1)
+        t = api.Trainer(init, sc.images, sc.extent, opt)
+        t.step(W)
+        t.synchronize()
+        log(f"launches_before={int(L.u3dg_launch_count())} launches_per_step_follow")
+        t.step(args.ncu_steps)
+        t.synchronize()
+        log(f"launches_after={int(L.u3dg_launch_count())}")
+        return None
     total_needed = W + K + args.profile_steps
     opt.iterations = max(opt.iterations, total_needed + 1)
     # --- device-timed throughput, inputs resident in HBM
@@ -205,10 +226,12 @@ def run_ours(args, dist: Dist) -> dict:
     dist.barrier()
     e0 = time.perf_counter()
     t2 = api.Trainer(init, sc.images, sc.extent, opt)
+    ec = time.perf_counter()
     t2.step(K)
     model = t2.model()
     st2 = t2.stats()
     e1 = time.perf_counter()
+    log(f"e2e: create {ec - e0:.3f} s, steps + download {e1 - ec:.3f} s")
     e2e_s = dist.max(e1 - e0)
     del t2
     image_bytes = sum(im.rgb.nbytes for im in sc.images)
@@ -261,7 +284,7 @@ def cpu_baseline(args, seconds: float = 15.0) -> dict:
         return {"value": None, "unit": "it/s", "kind": "reference", "cores": os.cpu_count(),
                 "sample": "unavailable: oracle/_ref not built"}
     ref = Reference()
-    sc, xyz, rgb, opt = build_workload(render_on_gpu=True, seed=0)
+    sc, xyz, rgb, opt = args.built
     init = ref.init_from_points(xyz, rgb)
     threads = ref.pool_threads(0)
     t = ref.trainer(init, sc.images, sc.extent, opt, threads=0)
@@ -285,7 +308,7 @@ def run_reference(args, dist: Dist) -> dict | None:
     if not Reference.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libu3dref.so is not built (reference sources absent)"}
     ref = Reference()
-    sc, xyz, rgb, opt = build_workload(render_on_gpu=False, seed=0)
+    sc, xyz, rgb, opt = build_workload(render_on_gpu=False, seed=0, workload=args.workload)
     init = ref.init_from_points(xyz, rgb)
     threads = ref.pool_threads(0)
     W, K = args.warmup, args.steps
@@ -305,8 +328,13 @@ def run_reference(args, dist: Dist) -> dict | None:
 
 
 def config(args, dist: Dist) -> dict:
-    return {"workload": "high-300k", "scene": "High preset (seed 0): 250k GT Gaussians, SH3, 150 views 640x480",
-            "model_gaussians": MODEL_CAP, "resolution": "640x480", "views": 150, "tile": 16,
+    from univeral_3d_reconstruction_system_b200.scenes import PRESETS
+    preset, cap = WORKLOADS[args.workload]
+    sp = PRESETS[preset]
+    return {"workload": args.workload,
+            "scene": f"{preset} preset (seed 0): {sp.gt_count} GT Gaussians, SH3, {sp.views} views "
+                     f"{sp.width}x{sp.height}",
+            "model_gaussians": cap, "resolution": f"{sp.width}x{sp.height}", "views": sp.views, "tile": 16,
             "phase": "steady (densification finished)", "parallelism": f"replicas x{dist.world}",
             "l2": "inputs larger than L2: per step the model, Adam moments and raster buffers (~0.3 GB) "
                   "exceed the 126 MB L2"}
@@ -321,6 +349,9 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="high-300k")
+    ap.add_argument("--ncu-steps", type=int, default=0,
+                    help="profiling run for ncu: warm up, log the launch count, run this many steps, exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     dist = Dist(args.gpus)
@@ -331,6 +362,8 @@ def main():
                 print(json.dumps(out), flush=True)
             return
         res = run_ours(args, dist)
+        if res is None:
+            return
         line = {"metric": METRIC, "value": res["value"], "unit": "it/s", "n_gpus": dist.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -193,6 +193,12 @@ int u3dg_trainer_synchronize(u3dg_trainer *trainer);
  * pair per phase and waits for each step; leave it off for throughput runs. */
 int u3dg_trainer_set_profiling(u3dg_trainer *trainer, int enable);
 int u3dg_trainer_phase_times(u3dg_trainer *trainer, u3dg_phase_times *out);
+/* Tile-Gaussian intersection buffers. Steps never wait for the GPU to learn their intersection count:
+ * a step that overflows the buffers does no update, and the trainer grows the buffers and replays it
+ * (bit-identical to a run that never overflowed). set_intersection_capacity sizes the buffers (they
+ * still grow on demand); replays reports how many steps were replayed so far. */
+int u3dg_trainer_set_intersection_capacity(u3dg_trainer *trainer, size_t capacity);
+int u3dg_trainer_replays(u3dg_trainer *trainer, int *replays);
 /* Device time in milliseconds of `count` steps, measured with CUDA events recorded on the
  * trainer's stream right before the first and after the last step (host waits on both sides). */
 int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms);

@@ -56,6 +56,8 @@ SIGNATURES = {
     "u3dg_trainer_set_profiling": (C.c_int, [_P, C.c_int]),
     "u3dg_trainer_phase_times": (C.c_int, [_P, C.POINTER(_abi.PhaseTimes)]),
     "u3dg_trainer_time_steps": (C.c_int, [_P, C.c_int, _F]),
+    "u3dg_trainer_set_intersection_capacity": (C.c_int, [_P, C.c_size_t]),
+    "u3dg_trainer_replays": (C.c_int, [_P, _I]),
     "u3dg_trainer_destroy": (None, [_P]),
     "u3dg_rasterizer_create": (C.c_int, [_PP]),
     "u3dg_rasterizer_forward": (C.c_int, [_P, _MV, _CAM, _ST, _F]),

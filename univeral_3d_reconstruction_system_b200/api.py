@@ -119,6 +119,14 @@ class Trainer:
         check(load().u3dg_trainer_time_steps(self._h, count, C.byref(ms)))
         return float(ms.value)
 
+    def set_intersection_capacity(self, capacity: int) -> None:
+        check(load().u3dg_trainer_set_intersection_capacity(self._h, int(capacity)))
+
+    def replays(self) -> int:
+        r = C.c_int()
+        check(load().u3dg_trainer_replays(self._h, C.byref(r)))
+        return r.value
+
     def set_profiling(self, enable: bool) -> None:
         check(load().u3dg_trainer_set_profiling(self._h, 1 if enable else 0))
 

@@ -8,22 +8,32 @@
 //   2. intersections are emitted in depth-rank order (an exclusive scan of per-rank tile counts
 //      gives each Gaussian its slots), keyed by tile id, and sorted stably by the tile id only.
 // Within a tile the emission order, i.e. (depth bits, id), survives, which is exactly the
-// reference's list. All sorts are stable 8-bit-digit LSD passes: per-block digit histograms, a
-// per-digit scan over blocks, and a scatter whose in-block ranks come from warp match-any votes.
+// reference's list.
+//
+// The intersection count is only known on the device, so nothing here waits for the host: item
+// counts are read from device memory, grids are sized for the capacity, and a capacity check turns
+// an overflow into an empty bin list plus a flag the host reads later (it then grows the buffers and
+// replays the step).
+//
+// Sorting: stable 8-bit-digit LSD passes. A pass is three kernels: per-block digit histograms, a
+// per-digit scan over the blocks, and a scatter whose in-block ranks come from warp match-any votes.
+// Every block owns one contiguous chunk of the items and walks it in rounds of kTile items.
 
 #include "kernels.h"
+
+#include <algorithm>
+#include <climits>
 
 namespace u3dg {
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItemsPerThread = 8;
-constexpr int kTile = kThreads * kItemsPerThread; // items per block
+constexpr int kItemsPerThread = 4;
+constexpr int kTile = kThreads * kItemsPerThread; // items per block round
 constexpr int kWarps = kThreads / 32;
 constexpr int kRadix = 256;
-
-inline int numBlocks(int n) { return (n + kTile - 1) / kTile; }
+constexpr int kMaxBlocks = 148 * 8;
 
 // Block-wide exclusive scan of one int per thread (blockDim == 256); returns the block total.
 __device__ __forceinline__ int blockExclusiveScan(int v, int &total)
@@ -58,33 +68,41 @@ __device__ __forceinline__ int blockExclusiveScan(int v, int &total)
     return before + x - v;
 }
 
-__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, int n, int shift, int *hist, int B)
+// The contiguous item range of block b when n items are split over G blocks in rounds of kTile.
+__device__ __forceinline__ void chunkOf(int n, int G, int b, int &begin, int &end)
+{
+    const long long per = (long long)G * kTile;
+    const int rounds = int((n + per - 1) / per);
+    const long long chunk = (long long)rounds * kTile;
+    begin = int(std::min<long long>(n, b * chunk));
+    end = int(std::min<long long>(n, begin + chunk));
+}
+
+__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int shift, int *hist,
+                                                            int G)
 {
     __shared__ int counts[kRadix];
     counts[threadIdx.x] = 0;
     __syncthreads();
-    const int base = blockIdx.x * kTile;
-#pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
-        const int i = base + r * kThreads + threadIdx.x;
-        if (i < n)
-            atomicAdd(&counts[(keys[i] >> shift) & 0xFF], 1);
-    }
+    int begin, end;
+    chunkOf(*nPtr, G, blockIdx.x, begin, end);
+    for (int i = begin + threadIdx.x; i < end; i += kThreads)
+        atomicAdd(&counts[(keys[i] >> shift) & 0xFF], 1);
     __syncthreads();
-    hist[threadIdx.x * B + blockIdx.x] = counts[threadIdx.x];
+    hist[threadIdx.x * G + blockIdx.x] = counts[threadIdx.x];
 }
 
-// One block per digit: exclusive scan of that digit's row of B block counts; rowTotals[d] = sum.
-__global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int B, int *rowTotals)
+// One block per digit: exclusive scan of that digit's row of G block counts; rowTotals[d] = sum.
+__global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G, int *rowTotals)
 {
-    int *row = hist + size_t(blockIdx.x) * B;
+    int *row = hist + size_t(blockIdx.x) * G;
     int carry = 0;
-    for (int c0 = 0; c0 < B; c0 += kThreads) {
+    for (int c0 = 0; c0 < G; c0 += kThreads) {
         const int i = c0 + threadIdx.x;
-        const int v = i < B ? row[i] : 0;
+        const int v = i < G ? row[i] : 0;
         int total;
         const int ex = blockExclusiveScan(v, total);
-        if (i < B)
+        if (i < G)
             row[i] = carry + ex;
         carry += total;
     }
@@ -93,74 +111,80 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int B,
 }
 
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
-                                                               uint32_t *keysOut, uint32_t *valsOut, int n, int shift,
-                                                               const int *hist, const int *rowTotals, int B)
+                                                               uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
+                                                               int shift, const int *hist, const int *rowTotals, int G)
 {
     __shared__ int warpCounts[kWarps][kRadix];
     __shared__ int base[kRadix];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = threadIdx.x; k < kWarps * kRadix; k += kThreads)
-        (&warpCounts[0][0])[k] = 0;
+    int begin, end;
+    chunkOf(*nPtr, G, blockIdx.x, begin, end);
     // Digit base: exclusive scan of the digit totals, plus this block's row prefix.
     {
         int total;
         const int ex = blockExclusiveScan(rowTotals[threadIdx.x], total);
-        base[threadIdx.x] = ex + hist[threadIdx.x * B + blockIdx.x];
+        base[threadIdx.x] = ex + hist[threadIdx.x * G + blockIdx.x];
     }
-    __syncthreads();
     const uint32_t lanesBelow = (1u << lane) - 1u;
-    const int first = blockIdx.x * kTile + warp * (32 * kItemsPerThread);
-    uint32_t key[kItemsPerThread], val[kItemsPerThread];
-    int digit[kItemsPerThread], local[kItemsPerThread];
+    for (int r0 = begin; r0 < end; r0 += kTile) {
+        for (int k = threadIdx.x; k < kWarps * kRadix; k += kThreads)
+            (&warpCounts[0][0])[k] = 0;
+        __syncthreads();
+        const int first = r0 + warp * (32 * kItemsPerThread);
+        uint32_t key[kItemsPerThread], val[kItemsPerThread];
+        int digit[kItemsPerThread], local[kItemsPerThread];
 #pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
-        const int i = first + r * 32 + lane;
-        const bool valid = i < n;
-        key[r] = valid ? keysIn[i] : 0u;
-        val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
-        const int d = valid ? int((key[r] >> shift) & 0xFF) : kRadix;
-        digit[r] = d;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        int before = 0;
-        if (valid) {
-            before = warpCounts[warp][d];
-            local[r] = before + __popc(peers & lanesBelow);
+        for (int r = 0; r < kItemsPerThread; ++r) {
+            const int i = first + r * 32 + lane;
+            const bool valid = i < end;
+            key[r] = valid ? keysIn[i] : 0u;
+            val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
+            const int d = valid ? int((key[r] >> shift) & 0xFF) : kRadix;
+            digit[r] = d;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            int before = 0;
+            if (valid) {
+                before = warpCounts[warp][d];
+                local[r] = before + __popc(peers & lanesBelow);
+            }
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1)
+                warpCounts[warp][d] = before + __popc(peers);
+            __syncwarp();
         }
-        __syncwarp();
-        if (valid && lane == __ffs(peers) - 1)
-            warpCounts[warp][d] = before + __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    // Exclusive prefix of every digit over the warps (warps hold consecutive item ranges).
-    {
-        int s = 0;
+        __syncthreads();
+        // Exclusive prefix of every digit over the warps (warps hold consecutive item ranges).
+        int roundTotal = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
             const int c = warpCounts[w][threadIdx.x];
-            warpCounts[w][threadIdx.x] = s;
-            s += c;
+            warpCounts[w][threadIdx.x] = roundTotal;
+            roundTotal += c;
         }
-    }
-    __syncthreads();
+        __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
-        const int d = digit[r];
-        if (d < kRadix) {
-            const int pos = base[d] + warpCounts[warp][d] + local[r];
-            keysOut[pos] = key[r];
-            valsOut[pos] = val[r];
+        for (int r = 0; r < kItemsPerThread; ++r) {
+            const int d = digit[r];
+            if (d < kRadix) {
+                const int pos = base[d] + warpCounts[warp][d] + local[r];
+                keysOut[pos] = key[r];
+                valsOut[pos] = val[r];
+            }
         }
+        __syncthreads();
+        base[threadIdx.x] += roundTotal;
     }
 }
 
-// Exclusive scan, reduce-then-scan.
+// Exclusive scan, reduce-then-scan over a host-known n.
+constexpr int kScanTile = kThreads * 8;
+
 __global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int n, int *partial)
 {
-    const int base = blockIdx.x * kTile;
+    const int base = blockIdx.x * kScanTile;
     int s = 0;
 #pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
+    for (int r = 0; r < 8; ++r) {
         const int i = base + r * kThreads + threadIdx.x;
         if (i < n)
             s += in[i];
@@ -189,19 +213,18 @@ __global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int 
 
 __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B)
 {
-    // Each thread owns kItemsPerThread consecutive items.
-    const int base = blockIdx.x * kTile + threadIdx.x * kItemsPerThread;
-    int v[kItemsPerThread];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * 8;
+    int v[8];
     int s = 0;
 #pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
+    for (int r = 0; r < 8; ++r) {
         v[r] = (base + r < n) ? in[base + r] : 0;
         s += v[r];
     }
     int total;
     int run = blockExclusiveScan(s, total) + partial[blockIdx.x];
 #pragma unroll
-    for (int r = 0; r < kItemsPerThread; ++r) {
+    for (int r = 0; r < 8; ++r) {
         if (base + r < n)
             out[base + r] = run;
         run += v[r];
@@ -226,46 +249,60 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
     cnt[r] = c;
 }
 
-// One thread per intersection: binary search of its rank in offs, then its tile in the rectangle
-// (row-major, as the reference's ty/tx loops).
-__global__ void emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
-                           uint32_t *keys, int *emitGid)
+// Capacity check of this bin pass: the usable count is the scan total, or 0 when it exceeds the
+// intersection buffers or a previous step already aborted (the abort is sticky until the host
+// clears it). iteration identifies the aborted step for the host.
+__global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int iteration)
 {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total)
-        return;
-    int lo = 0, hi = n; // last r with offs[r] <= e
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (offs[mid] <= e)
-            lo = mid;
-        else
-            hi = mid;
+    const int t = *total;
+    const bool over = t < 0 || t > capacity;
+    if (over) {
+        if (c->abortIter < 0)
+            c->abortIter = iteration;
+        c->need = max(c->need, t < 0 ? INT_MAX : t);
     }
-    const int g = int(sortedIds[lo]);
-    const int4 q = rect[g];
-    const int k = e - offs[lo];
-    const int w = q.z - q.x;
-    const int ty = q.y + k / w, tx = q.x + k % w;
-    keys[e] = uint32_t(ty * tilesX + tx);
-    emitGid[e] = g;
+    c->total = t;
+    c->effTotal = (over || c->abortIter >= 0) ? 0 : t;
 }
 
-__global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, int total, int *list, int *inv)
+// One thread per intersection (grid-stride): binary search of its rank in offs, then its tile in the
+// rectangle (row-major, as the reference's ty/tx loops).
+__global__ void emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c,
+                           int tilesX, uint32_t *keys, int *emitGid)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < total) {
-        const int e = int(sortedEmit[s]);
-        list[s] = emitGid[e];
-        inv[e] = s;
+    const int total = c->effTotal;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        int lo = 0, hi = n; // last r with offs[r] <= e
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (offs[mid] <= e)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const int g = int(sortedIds[lo]);
+        const int4 q = rect[g];
+        const int k = e - offs[lo];
+        const int w = q.z - q.x;
+        const int ty = q.y + k / w, tx = q.x + k % w;
+        keys[e] = uint32_t(ty * tilesX + tx);
+        emitGid[e] = g;
     }
 }
 
-__global__ void tileOffsetsKernel(const uint32_t *sortedKeys, int total, int tiles, int *tileOffsets)
+__global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c, int *list)
+{
+    const int total = c->effTotal;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x)
+        list[s] = emitGid[sortedEmit[s]];
+}
+
+__global__ void tileOffsetsKernel(const uint32_t *sortedKeys, const BinCounts *c, int tiles, int *tileOffsets)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > tiles)
         return;
+    const int total = c->effTotal;
     int lo = 0, hi = total; // first s with key >= t
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
@@ -281,36 +318,35 @@ inline int grid(long long n, int t) { return int((n + t - 1) / t); }
 
 } // namespace
 
-size_t radixHistEntries(int n) { return size_t(kRadix) * size_t(numBlocks(n) > 0 ? numBlocks(n) : 1); }
+int radixBlocks(int nMax) { return std::max(1, std::min(kMaxBlocks, (nMax + kTile - 1) / kTile)); }
 
-void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const uint32_t *valsIn, int n,
+size_t radixHistEntries(int nMax) { return size_t(kRadix) * size_t(radixBlocks(nMax)); }
+
+void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
                     int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s)
 {
     uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
-    const uint32_t *vin = valsIn;
-    const int B = numBlocks(n);
-    if (n > 0) {
-        for (int shift = 0; shift < bits; shift += 8) {
-            { radixHistKernel<<<B, kThreads, 0, s>>>(kin, n, shift, hist, B); countLaunch(); }
-            { radixRowScanKernel<<<kRadix, kThreads, 0, s>>>(hist, B, rowTotals); countLaunch(); }
-            { radixScatterKernel<<<B, kThreads, 0, s>>>(kin, vin, kout, vout, n, shift, hist, rowTotals, B); countLaunch(); }
-            // The output of this pass is the input of the next one.
-            uint32_t *nk = kin;
-            kin = kout;
-            kout = nk;
-            vin = vout;
-            vout = (vout == valsB) ? valsA : valsB;
-        }
+    const uint32_t *vin = nullptr;
+    const int G = radixBlocks(nMax);
+    for (int shift = 0; shift < bits; shift += 8) {
+        { radixHistKernel<<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
+        { radixRowScanKernel<<<kRadix, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
+        { radixScatterKernel<<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+        uint32_t *nk = kin;
+        kin = kout;
+        kout = nk;
+        vin = vout;
+        vout = (vout == valsB) ? valsA : valsB;
     }
     *keysOut = kin;
     *valsOut = const_cast<uint32_t *>(vin);
 }
 
-size_t scanPartialEntries(int n) { return size_t(numBlocks(n)) + 1; }
+size_t scanPartialEntries(int n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
 
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
 {
-    const int B = numBlocks(n);
+    const int B = (n + kScanTile - 1) / kScanTile;
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(int), s);
         return;
@@ -327,19 +363,33 @@ void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *ra
         { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, n, cnt, rankOf); countLaunch(); }
 }
 
-void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
-                uint32_t *keys, int *emitGid, cudaStream_t s)
+namespace {
+__global__ void setCountKernel(BinCounts *c, int n) { c->n = n; }
+} // namespace
+
+void launchSetCount(BinCounts *c, int n, cudaStream_t s)
 {
-    if (total > 0)
-        { emitKernel<<<grid(total, 256), 256, 0, s>>>(sortedIds, offs, rect, n, total, tilesX, keys, emitGid); countLaunch(); }
+    { setCountKernel<<<1, 1, 0, s>>>(c, n); countLaunch(); }
 }
 
-void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, int total, int tiles,
-                        int *list, int *inv, int *tileOffsets, cudaStream_t s)
+void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s)
 {
-    if (total > 0)
-        { finalizeKernel<<<grid(total, 256), 256, 0, s>>>(sortedEmit, emitGid, total, list, inv); countLaunch(); }
-    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, total, tiles, tileOffsets); countLaunch(); }
+    { capacityKernel<<<1, 1, 0, s>>>(total, capacity, c, iteration); countLaunch(); }
+}
+
+void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
+                int tilesX, uint32_t *keys, int *emitGid, cudaStream_t s)
+{
+    if (n > 0 && capacity > 0)
+        { emitKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, keys, emitGid); countLaunch(); }
+}
+
+void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
+                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s)
+{
+    if (capacity > 0)
+        { finalizeKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedEmit, emitGid, c, list); countLaunch(); }
+    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
 }
 
 } // namespace u3dg

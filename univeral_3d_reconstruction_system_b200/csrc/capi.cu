@@ -235,8 +235,8 @@ int u3dg_trainer_step(u3dg_trainer *trainer, int count)
 {
     return guarded([&] {
         TrainerImpl &t = impl(trainer);
-        for (int k = 0; k < count; ++k)
-            t.step();
+        if (count > 0)
+            t.stepTo(t.iteration + count);
     });
 }
 
@@ -264,7 +264,7 @@ int u3dg_trainer_stats(u3dg_trainer *trainer, u3dg_train_stats *out)
         TrainerImpl &t = impl(trainer);
         if (!out)
             throw StatusError(U3DG_ERR_INVALID_ARG, "out is NULL");
-        t.sync();
+        t.finish();
         out->iteration = t.iteration;
         out->loss = t.hStats.p->loss;
         out->psnr = t.hStats.p->psnr;
@@ -278,6 +278,7 @@ int u3dg_trainer_size(u3dg_trainer *trainer, size_t *count)
         TrainerImpl &t = impl(trainer);
         if (!count)
             throw StatusError(U3DG_ERR_INVALID_ARG, "count is NULL");
+        t.finish();
         *count = size_t(t.n);
     });
 }
@@ -286,6 +287,7 @@ int u3dg_trainer_download(u3dg_trainer *trainer, u3dg_model *out, size_t capacit
 {
     return guarded([&] {
         TrainerImpl &t = impl(trainer);
+        t.finish();
         if (count)
             *count = size_t(t.n);
         if (size_t(t.n) > capacity)
@@ -357,6 +359,30 @@ int u3dg_trainer_phase_times(u3dg_trainer *trainer, u3dg_phase_times *out)
     });
 }
 
+int u3dg_trainer_set_intersection_capacity(u3dg_trainer *trainer, size_t capacity)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        t.finish();
+        capacity = std::max<size_t>(capacity, 1024);
+        if (capacity > size_t(INT_MAX / 16))
+            throw StatusError(U3DG_ERR_CAPACITY, "capacity too large");
+        t.ws.iKeys0.release();
+        t.ws.icap = 0;
+        t.ws.reserveIntersections(capacity);
+    });
+}
+
+int u3dg_trainer_replays(u3dg_trainer *trainer, int *replays)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        if (!replays)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "replays is NULL");
+        *replays = t.replays;
+    });
+}
+
 int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms)
 {
     return guarded([&] {
@@ -366,10 +392,10 @@ int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms)
         cudaEvent_t a, b;
         U3DG_CUDA(cudaEventCreate(&a));
         U3DG_CUDA(cudaEventCreate(&b));
-        t.sync();
+        t.finish();
         U3DG_CUDA(cudaEventRecord(a, t.stream));
-        for (int k = 0; k < count; ++k)
-            t.step();
+        if (count > 0)
+            t.stepTo(t.iteration + count);
         U3DG_CUDA(cudaEventRecord(b, t.stream));
         U3DG_CUDA(cudaEventSynchronize(b));
         U3DG_CUDA(cudaEventElapsedTime(ms, a, b));
@@ -433,7 +459,7 @@ static void rasterForward(u3dg_rasterizer &r, const u3dg_model *model, const flo
         U3DG_CUDA(cudaMemcpyAsync(sh.p, shRest, model->count * K * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
         shDev = sh.p;
     }
-    r.ws.forward(r.model.params(), int(model->count), *camera, *settings, shDev, degree, s);
+    r.ws.forwardChecked(r.model.params(), int(model->count), *camera, *settings, shDev, degree, s);
     U3DG_CUDA(cudaGetLastError());
     U3DG_CUDA(cudaMemcpyAsync(rgb, r.ws.rgb.p, size_t(camera->width) * camera->height * 3 * sizeof(float),
                               cudaMemcpyDeviceToHost, s));
@@ -508,8 +534,10 @@ int u3dg_rasterizer_projection(u3dg_rasterizer *r, size_t n, float *mean2d, floa
         cudaStream_t s = R.stream.s;
         std::vector<SplatRec> rec(n);
         std::vector<int4> rc(n);
+        std::vector<float4> cv(n);
         if (n) {
             U3DG_CUDA(cudaMemcpyAsync(rec.data(), R.ws.rec.p, n * sizeof(SplatRec), cudaMemcpyDeviceToHost, s));
+            U3DG_CUDA(cudaMemcpyAsync(cv.data(), R.ws.cov2d.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
             U3DG_CUDA(cudaMemcpyAsync(rc.data(), R.ws.rect.p, n * sizeof(int4), cudaMemcpyDeviceToHost, s));
             if (depth)
                 U3DG_CUDA(cudaMemcpyAsync(depth, R.ws.depth.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -525,7 +553,7 @@ int u3dg_rasterizer_projection(u3dg_rasterizer *r, size_t n, float *mean2d, floa
             const SplatRec &q = rec[i];
             if (mean2d) { mean2d[2 * i] = vis ? q.mx : 0; mean2d[2 * i + 1] = vis ? q.my : 0; }
             if (conic) { conic[3 * i] = vis ? q.A : 0; conic[3 * i + 1] = vis ? q.B : 0; conic[3 * i + 2] = vis ? q.C : 0; }
-            if (cov2d) { cov2d[3 * i] = vis ? q.ca : 0; cov2d[3 * i + 1] = vis ? q.cb : 0; cov2d[3 * i + 2] = vis ? q.cc : 0; }
+            if (cov2d) { cov2d[3 * i] = vis ? cv[i].x : 0; cov2d[3 * i + 1] = vis ? cv[i].y : 0; cov2d[3 * i + 2] = vis ? cv[i].z : 0; }
             if (rgb) { rgb[3 * i] = vis ? q.r : 0; rgb[3 * i + 1] = vis ? q.g : 0; rgb[3 * i + 2] = vis ? q.b : 0; }
             if (alpha) alpha[i] = vis ? q.alpha : 0;
             if (depth && !vis) depth[i] = 0;
@@ -544,11 +572,11 @@ int u3dg_rasterizer_tiles(u3dg_rasterizer *r, int *tiles_x, int *tiles_y, int *o
         const size_t tiles = size_t(R.ws.tilesX) * R.ws.tilesY;
         if (tiles_x) *tiles_x = R.ws.tilesX;
         if (tiles_y) *tiles_y = R.ws.tilesY;
-        if (list_length) *list_length = size_t(R.ws.total);
+        if (list_length) *list_length = size_t(R.ws.total());
         cudaStream_t s = R.stream.s;
         if (offsets && offsets_capacity >= tiles + 1)
             U3DG_CUDA(cudaMemcpyAsync(offsets, R.ws.tileOffsets.p, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
-        const size_t L = std::min(list_capacity, size_t(R.ws.total));
+        const size_t L = std::min(list_capacity, size_t(R.ws.total()));
         if (list && L)
             U3DG_CUDA(cudaMemcpyAsync(list, R.ws.list.p, L * sizeof(int), cudaMemcpyDeviceToHost, s));
         R.stream.sync();
@@ -616,20 +644,32 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
                                   rc[i].x >= rc[i].z || rc[i].y >= rc[i].w))
                 throw StatusError(U3DG_ERR_INVALID_ARG, "rect of a visible Gaussian is outside the tile grid");
         }
-        if (n) {
-            U3DG_CUDA(cudaMemcpyAsync(ws.depthKey.p, keys.data(), n * 4, cudaMemcpyHostToDevice, st.s));
-            U3DG_CUDA(cudaMemcpyAsync(ws.rect.p, rc.data(), n * sizeof(int4), cudaMemcpyHostToDevice, st.s));
-            U3DG_CUDA(cudaMemcpyAsync(ws.radius.p, radius, n * sizeof(int), cudaMemcpyHostToDevice, st.s));
+        ws.reserveIntersections(std::max<size_t>(size_t(1) << 16, 4 * nn));
+        for (int attempt = 0;; ++attempt) {
+            // The depth sort overwrites its keys, so every attempt uploads them again.
+            if (n) {
+                U3DG_CUDA(cudaMemcpyAsync(ws.depthKey.p, keys.data(), n * 4, cudaMemcpyHostToDevice, st.s));
+                U3DG_CUDA(cudaMemcpyAsync(ws.rect.p, rc.data(), n * sizeof(int4), cudaMemcpyHostToDevice, st.s));
+                U3DG_CUDA(cudaMemcpyAsync(ws.radius.p, radius, n * sizeof(int), cudaMemcpyHostToDevice, st.s));
+            }
+            ws.clearCounts(st.s);
+            ws.bin(st.s, 0);
+            U3DG_CUDA(cudaGetLastError());
+            U3DG_CUDA(cudaMemcpyAsync(ws.hostCounts.p, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, st.s));
+            st.sync();
+            if (ws.hostCounts.p->abortIter < 0)
+                break;
+            if (attempt >= 8)
+                throw StatusError(U3DG_ERR_CAPACITY, "intersection buffers could not be sized");
+            ws.reserveIntersections(size_t(ws.hostCounts.p->need) + size_t(ws.hostCounts.p->need) / 4);
         }
-        ws.bin(st.s);
-        U3DG_CUDA(cudaGetLastError());
         const size_t tiles = size_t(tiles_x) * tiles_y;
         U3DG_CUDA(cudaMemcpyAsync(offsets, ws.tileOffsets.p, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost, st.s));
-        const size_t L = std::min(list_capacity, size_t(ws.total));
+        const size_t L = std::min(list_capacity, size_t(ws.total()));
         if (list && L)
             U3DG_CUDA(cudaMemcpyAsync(list, ws.list.p, L * sizeof(int), cudaMemcpyDeviceToHost, st.s));
         if (list_length)
-            *list_length = size_t(ws.total);
+            *list_length = size_t(ws.total());
         st.sync();
     });
 }
@@ -659,7 +699,7 @@ int u3dg_photometric_loss(const float *render, const float *target, int width, i
         U3DG_CUDA(cudaMemcpyAsync(dt.p, target, P * 12, cudaMemcpyHostToDevice, st.s));
         LossScratch ls{dabc.p, sums.p, blocks};
         launchLoss(dr.p, dt.p, nullptr, width, height, lambda, dg.p, ls, st.s);
-        launchLossFinalize(ls, width, height, lambda, nullptr, 0, vals.p, vals.p + 3, st.s);
+        launchLossFinalize(ls, width, height, lambda, nullptr, 0, nullptr, vals.p, vals.p + 3, st.s);
         U3DG_CUDA(cudaGetLastError());
         float v[4];
         U3DG_CUDA(cudaMemcpyAsync(v, vals.p, sizeof(v), cudaMemcpyDeviceToHost, st.s));
@@ -1022,7 +1062,7 @@ int u3dg_render_views_sh(const u3dg_model *model, const float *sh_rest, int degr
         for (int v = 0; v < count; ++v) {
             checkCamera(cameras[v]);
             const size_t P3 = size_t(cameras[v].width) * cameras[v].height * 3;
-            r.ws.forward(r.model.params(), int(model->count), cameras[v], *settings, shDev, degree, s);
+            r.ws.forwardChecked(r.model.params(), int(model->count), cameras[v], *settings, shDev, degree, s);
             q.reserve(P3);
             launchQuantize(r.ws.rgb.p, P3, q.p, s);
             U3DG_CUDA(cudaGetLastError());

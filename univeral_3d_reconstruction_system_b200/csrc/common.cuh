@@ -36,14 +36,17 @@ inline Params paramsAt(float *base, size_t capacity)
     return p;
 }
 
-// Raster record of one projected Gaussian (48 bytes, 16-byte aligned): what the compositing
-// kernels gather per tile-list entry, plus the 2D covariance kept for inspection.
+// Raster record of one projected Gaussian (48 bytes = 3 x float4): what the compositing kernels
+// gather per tile-list entry. (ex, ey) are the half-extents of a conservative axis-aligned box around
+// every pixel whose alpha can reach the minimum alpha; compositing warps skip the Gaussian when their
+// pixel block lies outside it (the tile lists themselves stay exactly the reference's).
 struct __align__(16) SplatRec {
-    float mx, my;      // projected mean (pixels)
-    float A, B, C;     // conic = inverse 2D covariance
-    float alpha;       // sigmoid(opacity)
-    float r, g, b;     // clamped DC colour
-    float ca, cb, cc;  // 2D covariance including eps2d
+    float mx, my;  // projected mean (pixels)
+    float ex, ey;  // contributing half-extents (pixels); +inf = no culling
+    float A, B, C; // conic = inverse 2D covariance
+    float alpha;   // sigmoid(opacity)
+    float r, g, b; // clamped DC colour
+    float depth;   // camera-space depth
 };
 
 // Per-step scalars the device computes and the host reads lazily.

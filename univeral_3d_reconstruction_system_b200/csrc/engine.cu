@@ -1,10 +1,14 @@
 // engine.cu - host orchestration of the GPU trainer: raster workspace, Trainer, densification.
 //
 // One CUDA stream per trainer. A step queues: projection, depth sort, per-rank tile counts + scan,
-// (one 4-byte read of the intersection count to size the intersection buffers), emission, tile
-// sort, tile offsets, compositing forward, loss forward/backward + stats, compositing backward, and
-// the chain rule fused with Adam. The training RNG (std::mt19937, Trainer.h:79) stays on the host so
-// the view order and the split samples are the reference's exactly.
+// capacity check, emission, tile sort, tile offsets, compositing forward, loss forward/backward +
+// stats, compositing backward, and the chain rule fused with Adam - with no host wait inside. The
+// host reads each step's bin counts back asynchronously and checks them kLag steps later; a step whose
+// intersections overflowed the buffers did no update (the device skips it and every later step), so
+// the host restores its own state to that step, grows the buffers and replays. Densification steps
+// wait for the GPU anyway (the split count decides how many samples the host RNG draws).
+// The training RNG (std::mt19937, Trainer.h:79) stays on the host so the view order and the split
+// samples are the reference's exactly.
 
 #include "engine.h"
 
@@ -39,6 +43,46 @@ void checkCamera(const u3dg_camera &cam)
 
 // ------------------------------------------------------------------ raster workspace
 
+RasterWorkspace::RasterWorkspace()
+{
+    counts.reserve(1, true);
+    hostCounts.reserve(1);
+    BinCounts c{};
+    c.abortIter = -1;
+    *hostCounts.p = c;
+    U3DG_CUDA(cudaMemcpy(counts.p, &c, sizeof(c), cudaMemcpyHostToDevice));
+}
+
+void RasterWorkspace::clearCounts(cudaStream_t stream)
+{
+    BinCounts c{};
+    c.abortIter = -1;
+    // A kernel-free, stream-ordered reset: copy from a pinned value that is never modified afterwards.
+    static thread_local HostPinned<BinCounts> zero;
+    if (!zero.p) {
+        zero.reserve(1);
+        *zero.p = c;
+    }
+    U3DG_CUDA(cudaMemcpyAsync(counts.p, zero.p, sizeof(BinCounts), cudaMemcpyHostToDevice, stream));
+}
+
+void RasterWorkspace::reserveIntersections(size_t capacity)
+{
+    capacity = std::max<size_t>(capacity, 1024);
+    if (capacity > size_t(INT_MAX / 16))
+        throw StatusError(U3DG_ERR_CAPACITY, "tile-Gaussian intersections exceed the supported 1.3e8");
+    if (int(capacity) <= icap && iKeys0.p)
+        return;
+    iKeys0.reserve(capacity, true);
+    iKeys1.reserve(capacity, true);
+    iVals0.reserve(capacity, true);
+    iVals1.reserve(capacity, true);
+    emitGid.reserve(capacity, true);
+    list.reserve(capacity, true);
+    partial.reserve(capacity * kG2d, true);
+    icap = int(capacity);
+}
+
 void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
                               const float *shRest, int shDegree, cudaStream_t stream)
 {
@@ -63,46 +107,51 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     offs.reserve(nn + 1);
     scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
     flags.reserve(nn);
-    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p};
+    cov2d.reserve(nn);
+    if (icap == 0)
+        reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * nn));
+    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
     launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream);
 }
 
-void RasterWorkspace::bin(cudaStream_t stream)
+void RasterWorkspace::bin(cudaStream_t stream, int iteration)
 {
     const int tiles = tilesX * tilesY;
-    hist.reserve(std::max(radixHistEntries(n), size_t(256)));
+    hist.reserve(std::max(radixHistEntries(std::max(n, icap)), size_t(256)));
     rowTotals.reserve(256);
+    tileOffsets.reserve(size_t(tiles) + 1);
     uint32_t *keysOut = nullptr, *valsOut = nullptr;
-    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, nullptr, n, 32, hist.p, rowTotals.p, &keysOut,
-                   &valsOut, stream);
+    launchSetCount(counts.p, n, stream);
+    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, &counts.p->n, std::max(n, 1), 32, hist.p,
+                   rowTotals.p, &keysOut, &valsOut, stream);
     sortedIds = valsOut;
     launchRankCounts(sortedIds, rect.p, radius.p, n, cnt.p, rankOf.p, stream);
     exclusiveScan(cnt.p, offs.p, n, scanPartial.p, stream);
-    hostTotal.reserve(1);
-    U3DG_CUDA(cudaMemcpyAsync(hostTotal.p, offs.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    U3DG_CUDA(cudaStreamSynchronize(stream));
-    total = *hostTotal.p;
-    if (total < 0)
-        throw StatusError(U3DG_ERR_CAPACITY, "tile-Gaussian intersection count overflowed 32 bits");
-    const size_t tt = size_t(std::max(total, 1));
-    iKeys0.reserve(tt);
-    iKeys1.reserve(tt);
-    iVals0.reserve(tt);
-    iVals1.reserve(tt);
-    emitGid.reserve(tt);
-    list.reserve(tt);
-    inv.reserve(tt);
-    partial.reserve(tt * kG2d);
-    hist.reserve(std::max(radixHistEntries(total), size_t(256)));
-    tileOffsets.reserve(size_t(tiles) + 1);
-    launchEmit(sortedIds, offs.p, rect.p, n, total, tilesX, iKeys0.p, emitGid.p, stream);
+    launchCapacityCheck(offs.p + n, icap, counts.p, iteration, stream);
+    launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, iKeys0.p, emitGid.p, stream);
     int bits = 0;
     while ((1 << bits) < tiles)
         ++bits;
     bits = std::max(bits, 1);
-    radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, nullptr, total, bits, hist.p, rowTotals.p, &keysOut,
-                   &valsOut, stream);
-    launchFinalizeBins(keysOut, valsOut, emitGid.p, total, tiles, list.p, inv.p, tileOffsets.p, stream);
+    radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits, hist.p, rowTotals.p,
+                   &keysOut, &valsOut, stream);
+    listEmit = valsOut;
+    launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p, stream);
+}
+
+void RasterWorkspace::forwardChecked(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
+                                     const float *shRest, int shDegree, cudaStream_t stream)
+{
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        clearCounts(stream);
+        forward(P, count, c, s, shRest, shDegree, stream, 0);
+        U3DG_CUDA(cudaMemcpyAsync(hostCounts.p, counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, stream));
+        U3DG_CUDA(cudaStreamSynchronize(stream));
+        if (hostCounts.p->abortIter < 0)
+            return;
+        reserveIntersections(size_t(hostCounts.p->need) + size_t(hostCounts.p->need) / 4);
+    }
+    throw StatusError(U3DG_ERR_CAPACITY, "intersection buffers could not be sized");
 }
 
 RasterArgs RasterWorkspace::rasterArgs() const
@@ -110,6 +159,7 @@ RasterArgs RasterWorkspace::rasterArgs() const
     RasterArgs a;
     a.tileOffsets = tileOffsets.p;
     a.list = list.p;
+    a.listEmit = listEmit;
     a.rec = rec.p;
     a.width = cam.width;
     a.height = cam.height;
@@ -133,8 +183,8 @@ void RasterWorkspace::composite(cudaStream_t stream)
 
 void RasterWorkspace::backwardComposite(const float *dLdRgb, cudaStream_t stream)
 {
-    if (st.tile_size > 16 && total > 0)
-        U3DG_CUDA(cudaMemsetAsync(partial.p, 0, size_t(total) * kG2d * sizeof(float), stream));
+    if (st.tile_size > 16)
+        U3DG_CUDA(cudaMemsetAsync(partial.p, 0, size_t(icap) * kG2d * sizeof(float), stream));
     launchCompositeBackward(rasterArgs(), dLdRgb, finalT.p, nContrib.p, partial.p, stream);
 }
 
@@ -150,8 +200,8 @@ ChainArgs RasterWorkspace::chainArgs(const Params &P) const
     a.flags = flags.p;
     a.rankOf = rankOf.p;
     a.offs = offs.p;
-    a.inv = inv.p;
     a.partial = partial.p;
+    a.counts = counts.p;
     return a;
 }
 
@@ -232,6 +282,9 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     U3DG_CUDA(cudaMemsetAsync(dStats.p, 0, sizeof(DevStats), stream));
     std::memset(hStats.p, 0, sizeof(DevStats));
     hCounts.reserve(4);
+    statusSlots.reserve(kSlots);
+    // Intersection buffers sized for 16 tiles per Gaussian at the capacity; they grow on demand.
+    ws.reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * cap));
     // The host buffers of the caller may be released after this call returns.
     U3DG_CUDA(cudaStreamSynchronize(stream));
 }
@@ -242,15 +295,101 @@ TrainerImpl::~TrainerImpl()
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
     }
+    for (InFlight &f : inflight)
+        cudaEventDestroy(f.done);
+    for (cudaEvent_t e : freeEvents)
+        cudaEventDestroy(e);
     delete timer;
 }
 
 void TrainerImpl::sync() { U3DG_CUDA(cudaStreamSynchronize(stream)); }
 
+HostSnapshot TrainerImpl::snapshot() const
+{
+    HostSnapshot s;
+    s.iteration = iteration;
+    s.orderPos = orderPos;
+    s.order = order;
+    s.rng = rng;
+    s.adamStep = adamStep;
+    s.opacityWasReset = opacityWasReset;
+    return s;
+}
+
+void TrainerImpl::restore(const HostSnapshot &s)
+{
+    iteration = s.iteration;
+    orderPos = s.orderPos;
+    order = s.order;
+    rng = s.rng;
+    adamStep = s.adamStep;
+    opacityWasReset = s.opacityWasReset;
+}
+
+bool TrainerImpl::checkOldest()
+{
+    InFlight f = inflight.front();
+    inflight.erase(inflight.begin());
+    U3DG_CUDA(cudaEventSynchronize(f.done));
+    freeEvents.push_back(f.done);
+    const BinCounts c = statusSlots.p[f.slot];
+    if (c.abortIter < 0) {
+        // Grow ahead of need: keep a quarter of headroom over the largest pass seen.
+        if (size_t(c.total) + size_t(c.total) / 4 > size_t(ws.icap)) {
+            sync();
+            ws.reserveIntersections(size_t(c.total) + size_t(c.total) / 2);
+        }
+        return true;
+    }
+    // This step overflowed: it and every step queued after it did nothing on the device.
+    sync();
+    for (InFlight &g : inflight)
+        freeEvents.push_back(g.done);
+    inflight.clear();
+    restore(f.snap);
+    ws.reserveIntersections(size_t(c.need) + size_t(c.need) / 2);
+    ws.clearCounts(stream);
+    ++replays;
+    return false;
+}
+
 void TrainerImpl::step()
 {
     if (cams.empty() || done())
         return;
+    while (int(inflight.size()) >= kLag)
+        if (!checkOldest())
+            return; // rolled back; the caller's loop replays from the restored iteration
+    enqueueStep();
+}
+
+void TrainerImpl::stepTo(int target)
+{
+    target = std::min(target, o.iterations);
+    while (iteration < target && !cams.empty())
+        step();
+}
+
+void TrainerImpl::finish()
+{
+    const int target = iteration;
+    for (;;) {
+        bool ok = true;
+        while (!inflight.empty())
+            if (!checkOldest()) {
+                ok = false;
+                break;
+            }
+        if (ok)
+            return;
+        stepTo(target);
+    }
+}
+
+void TrainerImpl::enqueueStep()
+{
+    InFlight f;
+    f.snap = snapshot();
     // View order: one shuffle of all views per epoch (Trainer.cpp:57-64).
     if (orderPos >= order.size()) {
         order.resize(cams.size());
@@ -269,7 +408,7 @@ void TrainerImpl::step()
     ws.project(params(), n, cam, o.raster, nullptr, 0, stream);
     if (tm)
         tm->mark(1, stream);
-    ws.bin(stream);
+    ws.bin(stream, iteration);
     if (tm)
         tm->mark(2, stream);
     ws.composite(stream);
@@ -280,7 +419,7 @@ void TrainerImpl::step()
     lossBlockSums.reserve(size_t(lb) * 3);
     LossScratch ls{abc.p, lossBlockSums.p, lb};
     launchLoss(ws.rgb.p, nullptr, target, W, H, o.ssim_lambda, dLoss.p, ls, stream);
-    launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, iteration + 1, nullptr, nullptr, stream);
+    launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, iteration + 1, ws.counts.p, nullptr, nullptr, stream);
     if (tm)
         tm->mark(4, stream);
     ws.backwardComposite(dLoss.p, stream);
@@ -307,8 +446,27 @@ void TrainerImpl::step()
     if (tm)
         tm->mark(6, stream);
     ++iteration;
-    if (iteration >= o.refine_start && iteration < o.refine_stop && iteration % o.refine_interval == 0)
-        densifyAndPrune();
+    f.slot = nextSlot;
+    nextSlot = (nextSlot + 1) % kSlots;
+    U3DG_CUDA(cudaMemcpyAsync(statusSlots.p + f.slot, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, stream));
+    if (freeEvents.empty()) {
+        cudaEvent_t e;
+        U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        freeEvents.push_back(e);
+    }
+    f.done = freeEvents.back();
+    freeEvents.pop_back();
+    U3DG_CUDA(cudaEventRecord(f.done, stream));
+    inflight.push_back(f);
+    if (iteration >= o.refine_start && iteration < o.refine_stop && iteration % o.refine_interval == 0) {
+        // The densification decision needs this step's statistics: finish (and replay) first. A replay
+        // inside finish() reaches this iteration again and densifies there; do not densify twice.
+        finish();
+        if (densifiedAt != iteration) {
+            densifyAndPrune();
+            densifiedAt = iteration;
+        }
+    }
     if (o.opacity_reset_interval > 0 && iteration < o.refine_stop && iteration % o.opacity_reset_interval == 0)
         resetOpacity();
     U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
@@ -325,7 +483,8 @@ void TrainerImpl::step()
         acc.update_ms += tm->between(5, 6);
         acc.densify_ms += tm->between(6, 7);
         acc.total_ms += tm->between(0, 7);
-        acc.intersections += uint64_t(ws.total);
+        U3DG_CUDA(cudaMemcpy(ws.hostCounts.p, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost));
+        acc.intersections += uint64_t(std::max(ws.hostCounts.p->effTotal, 0));
         acc.gaussians += uint64_t(ws.n);
         acc.pixels += uint64_t(W) * uint64_t(H);
     }
@@ -395,24 +554,28 @@ void TrainerImpl::densifyAndPrune()
     lastPruned = r.pruned;
     lastClones = r.clones;
     lastSplits = r.splits;
+    // More Gaussians usually means more intersections: keep 16 per Gaussian of headroom.
+    if (size_t(ws.icap) < 16 * size_t(n))
+        ws.reserveIntersections(16 * size_t(n));
 }
 
 void TrainerImpl::resetOpacity()
 {
     // logit(0.01f) in host float arithmetic (GaussianModel.h:13, Trainer.cpp:173).
     const float cap01 = std::log(0.01f / (1.0f - 0.01f));
-    launchOpacityReset(params().opac, moment1().opac, moment2().opac, n, cap01, stream);
+    launchOpacityReset(params().opac, moment1().opac, moment2().opac, n, cap01, ws.counts.p, stream);
     opacityWasReset = true;
 }
 
 float TrainerImpl::evaluatePsnr()
 {
+    finish();
     if (cams.empty())
         return 0.0f;
     constexpr int kSq = 297; // sqDiff partial blocks + 1 (loss.cu)
     psnrSums.reserve(cams.size() * kSq);
     for (size_t v = 0; v < cams.size(); ++v) {
-        ws.forward(params(), n, cams[v], o.raster, nullptr, 0, stream);
+        ws.forwardChecked(params(), n, cams[v], o.raster, nullptr, 0, stream);
         const size_t count = size_t(cams[v].width) * cams[v].height * 3;
         launchPsnrU8(ws.rgb.p, images.p + imageOffset[v], count, psnrSums.p + v * kSq, stream);
     }
@@ -430,7 +593,8 @@ float TrainerImpl::evaluatePsnr()
 
 void TrainerImpl::render(const u3dg_camera &c, float *hostRgb)
 {
-    ws.forward(params(), n, c, o.raster, nullptr, 0, stream);
+    finish();
+    ws.forwardChecked(params(), n, c, o.raster, nullptr, 0, stream);
     U3DG_CUDA(cudaMemcpyAsync(hostRgb, ws.rgb.p, size_t(c.width) * c.height * 3 * sizeof(float), cudaMemcpyDeviceToHost,
                               stream));
     sync();
@@ -438,6 +602,7 @@ void TrainerImpl::render(const u3dg_camera &c, float *hostRgb)
 
 void TrainerImpl::download(u3dg_model &out)
 {
+    finish();
     copyArenaToModel(arena[cur].p, cap, size_t(n), out, stream);
     sync();
 }

@@ -106,32 +106,49 @@ struct RasterWorkspace {
     DevBuf<int4> rect;
     DevBuf<int> radius, rankOf, cnt, offs, scanPartial, hist, rowTotals;
     DevBuf<uint8_t> flags;
-    // per intersection
+    DevBuf<float4> cov2d;
+    // per intersection (capacity icap)
     DevBuf<uint32_t> iKeys0, iKeys1, iVals0, iVals1;
-    DevBuf<int> emitGid, list, inv;
+    DevBuf<int> emitGid, list;
+    uint32_t *listEmit = nullptr; // emission index per tile-sorted entry (one of iVals0 / iVals1)
     DevBuf<float> partial;
+    int icap = 0;
     // per tile / pixel
     DevBuf<int> tileOffsets, nContrib;
     DevBuf<float> rgb, finalT;
-    HostPinned<int> hostTotal;
+    // device-side sizes of the last pass and their pinned host copy
+    DevBuf<BinCounts> counts;
+    HostPinned<BinCounts> hostCounts;
 
-    int n = 0, total = 0, tilesX = 0, tilesY = 0;
+    int n = 0, tilesX = 0, tilesY = 0;
     u3dg_camera cam{};
     u3dg_raster_settings st{};
     uint32_t *sortedIds = nullptr;
-    // Device-side event of the last binning readback (for profiling).
+
+    RasterWorkspace();
+    // Sizes the intersection buffers for `capacity` entries (waits for the device if they grow).
+    void reserveIntersections(size_t capacity);
+    // Clears the overflow / abort record (stream-ordered).
+    void clearCounts(cudaStream_t stream);
     void project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
                  int shDegree, cudaStream_t stream);
-    // Depth sort + tile binning from depthKey / rect / radius (waits for the intersection count).
-    void bin(cudaStream_t stream);
+    // Depth sort + tile binning from depthKey / rect / radius. Never waits for the device: an overflow of
+    // the intersection buffers is recorded in `counts` (tagged with `iteration`) and bins nothing.
+    void bin(cudaStream_t stream, int iteration);
     void composite(cudaStream_t stream);
     void forward(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
-                 int shDegree, cudaStream_t stream)
+                 int shDegree, cudaStream_t stream, int iteration)
     {
         project(P, count, c, s, shRest, shDegree, stream);
-        bin(stream);
+        bin(stream, iteration);
         composite(stream);
     }
+    // A forward that is complete when it returns: waits, and on an overflow grows the intersection
+    // buffers and runs again. For the unit entry points and evaluation, not the training loop.
+    void forwardChecked(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
+                        const float *shRest, int shDegree, cudaStream_t stream);
+    // Intersections binned by the last completed pass (valid after a wait).
+    int total() const { return hostCounts.p->effTotal; }
     // Compositing backward into `partial`.
     void backwardComposite(const float *dLdRgb, cudaStream_t stream);
     RasterArgs rasterArgs() const;
@@ -162,6 +179,22 @@ struct PhaseTimer {
     }
 };
 
+// Host-side trainer state before a step: what a replay restores.
+struct HostSnapshot {
+    int iteration = 0;
+    size_t orderPos = 0;
+    std::vector<int> order;
+    std::mt19937 rng;
+    int adamStep = 0;
+    bool opacityWasReset = false;
+};
+
+// A queued step whose device-side status has not been checked yet.
+struct InFlight {
+    HostSnapshot snap;
+    cudaEvent_t done = nullptr;
+    int slot = 0; // pinned status slot
+};
 
 // The GPU Trainer (Trainer.h:47-93, Trainer.cpp).
 struct TrainerImpl {
@@ -196,6 +229,16 @@ struct TrainerImpl {
     int adamStep = 0;
     bool opacityWasReset = false;
     int lastPruned = 0, lastClones = 0, lastSplits = 0;
+    int replays = 0;                  // steps replayed after an intersection-buffer overflow
+    int densifiedAt = -1;             // iteration of the last densification
+
+    // Steps run ahead of their status check by at most kLag steps.
+    static constexpr int kLag = 2;
+    static constexpr int kSlots = 8;
+    std::vector<InFlight> inflight;
+    std::vector<cudaEvent_t> freeEvents;
+    HostPinned<BinCounts> statusSlots; // kSlots pinned copies of the bin counts, one per queued step
+    int nextSlot = 0;
 
     bool profiling = false;
     PhaseTimer *timer = nullptr;
@@ -210,13 +253,25 @@ struct TrainerImpl {
     Params paramsOf(int which, int k) { return paramsAt(arena[which].p + size_t(k) * 14 * cap, cap); }
 
     bool done() const { return iteration >= o.iterations; }
+    // Trainer::step: queues one step (after checking the step kLag before it).
     void step();
+    // Runs steps until `target` iterations are reached (or done), replaying after overflows.
+    void stepTo(int target);
+    // Waits for every queued step and replays any that overflowed; afterwards the state is final.
+    void finish();
     void densifyAndPrune();
     void resetOpacity();
     float evaluatePsnr();
     void render(const u3dg_camera &c, float *hostRgb);
     void download(u3dg_model &out);
     void sync();
+
+private:
+    HostSnapshot snapshot() const;
+    void restore(const HostSnapshot &s);
+    void enqueueStep();
+    // Checks the oldest queued step; returns false (after rolling back) when it had overflowed.
+    bool checkOldest();
 };
 
 // Densification on device arrays (shared by the trainer and the unit entry point).

@@ -16,6 +16,7 @@ namespace u3dg {
 namespace {
 
 __device__ __forceinline__ float stdMax(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float mid2(const Ewa &p) { return 0.5f * (p.a + p.c); }
 
 // Degree 1..3 real-SH colour terms, 3DGS sign convention; coef points at 15 * 3 floats.
 __device__ float shRest(const float *coef, int degree, int ch, const float d[3])
@@ -105,9 +106,7 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
     SplatRec r;
     r.mx = u;
     r.my = v;
-    r.ca = p.a;
-    r.cb = p.b;
-    r.cc = p.c;
+    r.depth = p.pc[2];
     r.A = p.c * invDet;
     r.B = -p.b * invDet;
     r.C = p.a * invDet;
@@ -138,7 +137,26 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
     r.g = col3[1];
     r.b = col3[2];
     r.alpha = sigmoidCR(P.opac[i]);
+    // Contributing box: alpha = min(0.99, a exp(-q/2)) >= minAlpha  <=>  q <= t = 2 ln(a / minAlpha), and
+    // {q <= t} lies within |dx| <= sqrt(t Sxx), |dy| <= sqrt(t Syy). The float evaluation of q in the
+    // compositing kernels may differ from the exact q by a few ulps times the covariance condition
+    // number, so t is widened by 2% (enough up to a condition number of 1e4; beyond that, no culling)
+    // and the box by one pixel.
+    {
+        const float disc = stdMax(0.0f, mid2(p) * mid2(p) - det);
+        const float lmax = mid2(p) + sqrtf(disc), lmin = mid2(p) - sqrtf(disc);
+        const float minA = st.min_alpha;
+        if (minA > 0.0f && lmin > 0.0f && lmax <= 1e4f * lmin) {
+            const float t = 2.0f * logf(r.alpha / minA);
+            const float tt = stdMax(t, 0.0f) * 1.02f + 1e-5f;
+            r.ex = sqrtf(tt * p.a) + 1.0f;
+            r.ey = sqrtf(tt * p.c) + 1.0f;
+        } else {
+            r.ex = r.ey = __int_as_float(0x7f800000);
+        }
+    }
     out.rec[i] = r;
+    out.cov2d[i] = make_float4(p.a, p.b, p.c, 0.0f);
     out.flags[i] = f;
     out.rect[i] = rect;
     out.radius[i] = radius;
@@ -162,7 +180,7 @@ template <bool kAdam>
 __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n)
+    if (i >= a.n || (a.counts != nullptr && a.counts->abortIter >= 0))
         return;
     const Params &P = a.params;
     float gMeans[3] = {0, 0, 0}, gScales[3] = {0, 0, 0}, gQuats[4] = {0, 0, 0, 0}, gOpac = 0, gColors[3] = {0, 0, 0};
@@ -174,7 +192,7 @@ __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
         for (int k = 0; k < kG2d; ++k)
             g[k] = 0.0f;
         for (int e = e0; e < e1; ++e) {
-            const float *src = a.partial + size_t(a.inv[e]) * kG2d;
+            const float *src = a.partial + size_t(e) * kG2d;
 #pragma unroll
             for (int k = 0; k < kG2d; ++k)
                 g[k] += src[k];
@@ -464,9 +482,11 @@ __global__ void densifyWriteKernel(Params P, Params M, Params V, Params P2, Para
 }
 
 // Trainer::resetOpacity (Trainer.cpp:171-178): opacity = std::min(opacity, cap); opacity moments = 0.
-__global__ void opacityResetKernel(float *opac, float *mOpac, float *vOpac, int n, float cap)
+__global__ void opacityResetKernel(float *opac, float *mOpac, float *vOpac, int n, float cap, const BinCounts *counts)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (counts != nullptr && counts->abortIter >= 0)
+        return;
     if (i < n) {
         const float o = opac[i];
         opac[i] = (cap < o) ? cap : o;
@@ -536,10 +556,11 @@ void launchDensifyWrite(const Params &P, const Params &M, const Params &V, const
                                                       splitScan, keptTotal, normals, log16); countLaunch(); }
 }
 
-void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float cap, cudaStream_t s)
+void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float cap, const BinCounts *counts,
+                        cudaStream_t s)
 {
     if (n > 0)
-        { opacityResetKernel<<<blocks(n, 256), 256, 0, s>>>(opac, mOpac, vOpac, n, cap); countLaunch(); }
+        { opacityResetKernel<<<blocks(n, 256), 256, 0, s>>>(opac, mOpac, vOpac, n, cap, counts); countLaunch(); }
 }
 
 } // namespace u3dg

@@ -5,6 +5,17 @@
 
 namespace u3dg {
 
+// Device-side sizes of one bin pass. The host never waits for them inside a step: it reads the
+// struct back asynchronously and checks it one step later.
+struct BinCounts {
+    int n;         // Gaussians in the pass (input of the depth sort)
+    int total;     // tile-Gaussian intersections found by the scan
+    int effTotal;  // intersections actually binned: total, or 0 after an overflow / abort
+    int abortIter; // -1, or the first step whose intersections did not fit (sticky until cleared)
+    int need;      // largest intersection count that did not fit
+    int pad[3];
+};
+
 // Outputs of the projection kernel, one entry per Gaussian.
 struct ProjOut {
     SplatRec *rec;      // raster record (valid where radius > 0)
@@ -13,6 +24,7 @@ struct ProjOut {
     int4 *rect;         // tile rectangle x0, y0, x1, y1 (exclusive)
     int *radius;        // 0 = not visible
     uint8_t *flags;     // bit0/1: J clamped in x/y; bit2..4: colour clamped
+    float4 *cov2d;      // 2D covariance a, b, c (including eps2d), for inspection
 };
 
 // Arguments of the chain-rule kernel (backward pass 2), optionally fused with Adam.
@@ -26,8 +38,8 @@ struct ChainArgs {
     const uint8_t *flags;
     const int *rankOf;    // depth rank of every Gaussian
     const int *offs;      // per rank: first intersection in emission order (n + 1 entries)
-    const int *inv;       // emission index -> tile-sorted index
-    const float *partial; // per tile-sorted intersection: 9 summed 2D gradients
+    const float *partial; // per intersection, in emission order: 9 summed 2D gradients
+    const BinCounts *counts; // the kernel does nothing when counts->abortIter >= 0
     float *gradAccum;     // |dL/dmean2d| NDC statistic (may be null)
     int *gradCount;       // visibility count (may be null)
     Params grads;         // non-Adam mode: gradients are added here
@@ -51,15 +63,18 @@ void launchDensifyWrite(const Params &P, const Params &M, const Params &V, const
                         const Params &V2, int n, const int *keep, const int *keepScan, const int *accCost,
                         const int *accScan, const int *isSplit, const int *splitScan, int keptTotal,
                         const float *normals, float log16, cudaStream_t s);
-void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float cap, cudaStream_t s);
+// Skipped when counts (may be null) records an aborted step.
+void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float cap, const BinCounts *counts,
+                        cudaStream_t s);
 
 // binning.cu
-// Scratch needed by radixSortPairs for n items: two key and two value buffers of n entries plus
-// the histogram of radixHistEntries(n) ints.
-size_t radixHistEntries(int n);
-// Stable LSD radix sort of (key, value) pairs on key bits [0, bits); values == nullptr means the
-// initial values are the item indices. Result in *keysOut / *valsOut (one of the two buffers).
-void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const uint32_t *valsIn, int n,
+// Blocks of a radix pass sized for at most nMax items, and the histogram entries it needs.
+int radixBlocks(int nMax);
+size_t radixHistEntries(int nMax);
+// Stable LSD radix sort of (key, value) pairs on key bits [0, bits); the item count is read on the
+// device from *nDev (at most nMax); the initial values are the item indices. Result in *keysOut /
+// *valsOut (one of the two buffers).
+void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
                     int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s);
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
@@ -67,24 +82,28 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
 // Per depth rank: tile count of the Gaussian and the inverse map gid -> rank.
 void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt, int *rankOf,
                       cudaStream_t s);
+// Sets counts->n and checks *total against the intersection capacity (see BinCounts).
+void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s);
+void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 // Emission of the intersections in depth-rank order: tile key and Gaussian id per intersection.
-void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, int total, int tilesX,
-                uint32_t *keys, int *emitGid, cudaStream_t s);
-// After the tile sort: Gaussian id per sorted entry, inverse permutation, tile offsets.
-void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, int total, int tiles,
-                        int *list, int *inv, int *tileOffsets, cudaStream_t s);
+void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
+                int tilesX, uint32_t *keys, int *emitGid, cudaStream_t s);
+// After the tile sort: Gaussian id per sorted entry and the tile offsets.
+void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
+                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s);
 
 // raster.cu
 struct RasterArgs {
     const int *tileOffsets;
-    const int *list;
+    const int *list;          // Gaussian id per tile-sorted entry
+    const uint32_t *listEmit; // emission index per tile-sorted entry (where backward stores partials)
     const SplatRec *rec;
     int width, height, tileSize, tilesX;
     float bg[3];
     float minAlpha, minTransmittance;
 };
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s);
-// partial: 9 floats per tile-sorted entry; zeroed by the caller when tileSize > 16 (atomics).
+// partial: 9 floats per intersection in emission order; zeroed by the caller when tileSize > 16.
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
                              float *partial, cudaStream_t s);
 
@@ -99,9 +118,10 @@ int lossBlocks(int width, int height);
 void launchLoss(const float *render, const float *targetF, const uint8_t *targetU8, int width, int height, float lambda,
                 float *grad, const LossScratch &ls, cudaStream_t s);
 // Reduces the block sums into the step's LossValue / PSNR and updates the EMA stats
-// (Trainer.cpp:88-92). out3 (may be null) gets total, l1, ssim; psnrOut (may be null) the PSNR.
+// (Trainer.cpp:88-92) unless counts (may be null) records an aborted step. out3 (may be null) gets
+// total, l1, ssim; psnrOut (may be null) the PSNR.
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
-                        float *out3, float *psnrOut, cudaStream_t s);
+                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s);
 // PSNR of the render against a uint8 target, accumulated in double (evaluatePsnr).
 void launchPsnrU8(const float *render, const uint8_t *target, size_t count, double *sumOut, cudaStream_t s);
 void launchPsnrF(const float *a, const float *b, size_t count, double *sumOut, cudaStream_t s);

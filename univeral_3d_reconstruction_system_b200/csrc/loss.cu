@@ -220,9 +220,11 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
 
 // Single block: fixed-order sum of the block partials, LossValue, PSNR and the EMA stats.
 __global__ void __launch_bounds__(kThreads) lossFinalizeKernel(const double *blockSums, int blocks, int W, int H,
-                                                               float lambda, DevStats *stats, int iteration, float *out3,
-                                                               float *psnrOut)
+                                                               float lambda, DevStats *stats, int iteration,
+                                                               const BinCounts *counts, float *out3, float *psnrOut)
 {
+    if (counts != nullptr && counts->abortIter >= 0)
+        stats = nullptr; // an aborted step leaves the statistics alone (it is replayed)
     double s0 = 0, s1 = 0, s2 = 0;
     for (int b = threadIdx.x; b < blocks; b += kThreads) {
         s0 += blockSums[3 * b];
@@ -337,10 +339,10 @@ void launchLoss(const float *render, const float *targetF, const uint8_t *target
 }
 
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
-                        float *out3, float *psnrOut, cudaStream_t s)
+                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s)
 {
-    { lossFinalizeKernel<<<1, kThreads, 0, s>>>(ls.blockSums, ls.blocks, width, height, lambda, stats, iteration, out3,
-                                              psnrOut); countLaunch(); }
+    { lossFinalizeKernel<<<1, kThreads, 0, s>>>(ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
+                                              counts, out3, psnrOut); countLaunch(); }
 }
 
 void launchPsnrU8(const float *render, const uint8_t *target, size_t count, double *sumOut, cudaStream_t s)

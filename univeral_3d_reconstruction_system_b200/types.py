@@ -19,6 +19,7 @@ import numpy as np
 from . import _abi
 
 SH_C0 = 0.28209479177387814  # GaussianModel.h:10
+GROUPS_ORDER = ("means", "scales", "quats", "opacities", "colors")
 
 
 def sigmoid(x):
@@ -176,6 +177,25 @@ class TrainOptions:
 
     def replace(self, **kw) -> "TrainOptions":
         return dataclasses.replace(self, **kw)
+
+    @classmethod
+    def from_struct(cls, o: _abi.TrainOptions) -> "TrainOptions":
+        r = o.raster
+        return cls(o.iterations, o.max_gaussians, o.ssim_lambda,
+                   LearningRates(o.lr.means, o.lr.scales, o.lr.quats, o.lr.opacities, o.lr.colors),
+                   o.means_lr_final, o.densify_grad_threshold, o.percent_dense, o.refine_start, o.refine_stop,
+                   o.refine_interval, o.opacity_reset_interval, o.prune_opacity, o.seed,
+                   RasterSettings(r.tile_size, r.near_plane, r.eps2d, tuple(r.background), r.min_alpha,
+                                  r.min_transmittance))
+
+    def struct_tuple(self) -> tuple:
+        """Every field as stored in the C struct (float32 rounding applied), for comparisons."""
+        o = self.struct()
+        r = o.raster
+        return (o.iterations, o.max_gaussians, o.ssim_lambda, o.lr.means, o.lr.scales, o.lr.quats, o.lr.opacities,
+                o.lr.colors, o.means_lr_final, o.densify_grad_threshold, o.percent_dense, o.refine_start,
+                o.refine_stop, o.refine_interval, o.opacity_reset_interval, o.prune_opacity, o.seed, r.tile_size,
+                r.near_plane, r.eps2d, tuple(r.background), r.min_alpha, r.min_transmittance)
 
 
 @dataclass
