@@ -46,19 +46,26 @@ def log(*a):
 
 
 class Dist:
-    def __init__(self, gpus: int):
+    """One process per GPU (torchrun env vars). The process group is plumbing only: a barrier around
+    the timed region and the max over ranks of the measured times. NCCL on GPUs; gloo for CPU tests."""
+
+    def __init__(self, gpus: int, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = backend or "nccl"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
@@ -69,13 +76,20 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def aggregate_rate(steps_per_rank: int, world: int, max_seconds: float) -> float:
+    """Whole-job steps/s of `world` replicas that each ran `steps_per_rank` steps (weak scaling), timed by
+    the slowest rank."""
+    return world * steps_per_rank / max_seconds
 
 
 # ------------------------------------------------------------------ clocks
@@ -251,7 +265,7 @@ def run_ours(args, dist: Dist) -> dict:
     step_bytes = sum(bytes_.values())
     per_step_ms = ms / K
     res = {
-        "value": dist.world * K / (ms * 1e-3),
+        "value": aggregate_rate(K, dist.world, ms * 1e-3),
         "ms_per_step": per_step_ms,
         "gpu_launches": launches,
         "clocks": clock_info,
@@ -263,7 +277,7 @@ def run_ours(args, dist: Dist) -> dict:
             "step_bytes": step_bytes, "step_achieved_gbs": round(step_bytes / (per_step_ms * 1e-3) / 1e9, 1),
         },
         "e2e": {
-            "value": dist.world * K / e2e_s, "unit": "it/s",
+            "value": aggregate_rate(K, dist.world, e2e_s), "unit": "it/s",
             "h2d_bytes_per_step": int((image_bytes + model_bytes) / K),
             "d2h_bytes_per_step": int((model.size() * 56) / K + 32),
             "includes": "trainer creation from host arrays (images + model upload), K steps, model download",

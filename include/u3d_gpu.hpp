@@ -1,0 +1,344 @@
+// u3d_gpu.hpp - C++ drop-in for the reference's splat trainer API, over the C ABI of u3dg.h.
+//
+// Same types, names and semantics as engine/include/u3d/splat (Trainer.h, Rasterizer.h, Loss.h,
+// GaussianModel.h, SplatPly.h) of Abner0907/univeral_3d_reconstruction_system, in namespace u3d::gpu.
+// Header-only; link against libu3dg.so. Errors of the GPU library throw u3d::gpu::Error (the reference
+// has no error channel except the bool results of the PLY functions, which are kept).
+//
+// The constructors and fromReference/toReference helpers are templates over any type with the
+// reference's field names, so code holding the reference's own u3d::GaussianModel / TrainImage /
+// TrainOptions / RenderCamera can pass them straight in.
+#pragma once
+
+#include "u3dg.h"
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace u3d {
+namespace gpu {
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(int status)
+{
+    if (status != U3DG_OK)
+        throw Error(status, u3dg_last_error());
+}
+
+constexpr float kShC0 = 0.28209479177387814f; // GaussianModel.h:10
+
+// GaussianModel (GaussianModel.h:23-37).
+struct GaussianModel {
+    std::vector<float> means, scales, quats, opacities, colors;
+    std::size_t size() const { return opacities.size(); }
+    void resize(std::size_t n)
+    {
+        means.resize(n * 3);
+        scales.resize(n * 3);
+        quats.resize(n * 4);
+        opacities.resize(n);
+        colors.resize(n * 3);
+    }
+    u3dg_model view() const
+    {
+        return {const_cast<float *>(means.data()), const_cast<float *>(scales.data()),
+                const_cast<float *>(quats.data()), const_cast<float *>(opacities.data()),
+                const_cast<float *>(colors.data()), size()};
+    }
+};
+
+// RenderCamera / RasterSettings (Rasterizer.h:13-32).
+struct RenderCamera : u3dg_camera {
+    RenderCamera() : u3dg_camera{0, 0, 0, 0, 0, 0, {1, 0, 0, 0, 1, 0, 0, 0, 1}, {0, 0, 0}} {}
+};
+
+struct RasterSettings : u3dg_raster_settings {
+    RasterSettings() : u3dg_raster_settings{} { u3dg_raster_settings_default(this); }
+};
+
+struct LearningRates : u3dg_learning_rates {
+    LearningRates() : u3dg_learning_rates{1.6e-4f, 5e-3f, 1e-3f, 5e-2f, 2.5e-3f} {}
+};
+
+// TrainOptions (Trainer.h:20-38).
+struct TrainOptions : u3dg_train_options {
+    TrainOptions() : u3dg_train_options{} { u3dg_train_options_default(this); }
+    static TrainOptions forIterations(int iterations)
+    {
+        TrainOptions o;
+        u3dg_train_options_for_iterations(iterations, &o);
+        return o;
+    }
+};
+
+// TrainImage (Trainer.h:13-18).
+struct TrainImage {
+    RenderCamera camera;
+    std::vector<std::uint8_t> rgb; // height * width * 3
+};
+
+// TrainStats (Trainer.h:40-45).
+struct TrainStats {
+    int iteration = 0;
+    float loss = 0;
+    float psnr = 0;
+    std::size_t gaussians = 0;
+};
+
+// ------------------------------------------------------------------ adapters from / to reference types
+
+template <class Cam>
+RenderCamera cameraFrom(const Cam &c)
+{
+    RenderCamera r;
+    r.width = c.width;
+    r.height = c.height;
+    r.fx = c.fx;
+    r.fy = c.fy;
+    r.cx = c.cx;
+    r.cy = c.cy;
+    for (int k = 0; k < 9; ++k)
+        r.R[k] = c.R[k];
+    for (int k = 0; k < 3; ++k)
+        r.t[k] = c.t[k];
+    return r;
+}
+
+template <class M>
+GaussianModel modelFrom(const M &m)
+{
+    GaussianModel g;
+    g.means.assign(m.means.begin(), m.means.end());
+    g.scales.assign(m.scales.begin(), m.scales.end());
+    g.quats.assign(m.quats.begin(), m.quats.end());
+    g.opacities.assign(m.opacities.begin(), m.opacities.end());
+    g.colors.assign(m.colors.begin(), m.colors.end());
+    return g;
+}
+
+template <class M>
+M modelTo(const GaussianModel &g)
+{
+    M m;
+    m.means.assign(g.means.begin(), g.means.end());
+    m.scales.assign(g.scales.begin(), g.scales.end());
+    m.quats.assign(g.quats.begin(), g.quats.end());
+    m.opacities.assign(g.opacities.begin(), g.opacities.end());
+    m.colors.assign(g.colors.begin(), g.colors.end());
+    return m;
+}
+
+template <class O>
+TrainOptions optionsFrom(const O &o)
+{
+    TrainOptions t;
+    t.iterations = o.iterations;
+    t.max_gaussians = o.maxGaussians;
+    t.ssim_lambda = o.ssimLambda;
+    t.lr.means = o.lr.means;
+    t.lr.scales = o.lr.scales;
+    t.lr.quats = o.lr.quats;
+    t.lr.opacities = o.lr.opacities;
+    t.lr.colors = o.lr.colors;
+    t.means_lr_final = o.meansLrFinal;
+    t.densify_grad_threshold = o.densifyGradThreshold;
+    t.percent_dense = o.percentDense;
+    t.refine_start = o.refineStart;
+    t.refine_stop = o.refineStop;
+    t.refine_interval = o.refineInterval;
+    t.opacity_reset_interval = o.opacityResetInterval;
+    t.prune_opacity = o.pruneOpacity;
+    t.seed = o.seed;
+    t.raster.tile_size = o.raster.tileSize;
+    t.raster.near_plane = o.raster.nearPlane;
+    t.raster.eps2d = o.raster.eps2d;
+    for (int k = 0; k < 3; ++k)
+        t.raster.background[k] = o.raster.background[k];
+    t.raster.min_alpha = o.raster.minAlpha;
+    t.raster.min_transmittance = o.raster.minTransmittance;
+    return t;
+}
+
+inline TrainOptions optionsFrom(const TrainOptions &o) { return o; }
+
+template <class I>
+TrainImage imageFrom(const I &img)
+{
+    TrainImage t;
+    t.camera = cameraFrom(img.camera);
+    t.rgb.assign(img.rgb.begin(), img.rgb.end());
+    return t;
+}
+
+inline TrainImage imageFrom(const TrainImage &img) { return img; }
+inline GaussianModel modelFrom(const GaussianModel &m) { return m; }
+
+// ------------------------------------------------------------------ Trainer (Trainer.h:47-93)
+
+class Trainer
+{
+public:
+    // Trainer(GaussianModel initial, std::vector<TrainImage> images, float sceneExtent,
+    //         const TrainOptions &options, ThreadPool &pool). The pool is accepted for API
+    // compatibility and not used: the work runs on the current CUDA device.
+    template <class Model, class Image, class Options, class Pool>
+    Trainer(const Model &initial, const std::vector<Image> &images, float sceneExtent, const Options &options, Pool &)
+        : Trainer(modelFrom(initial), convert(images), sceneExtent, optionsFrom(options))
+    {
+    }
+
+    Trainer(GaussianModel initial, std::vector<TrainImage> images, float sceneExtent, const TrainOptions &options)
+        : m_images(std::move(images)), m_options(options)
+    {
+        std::vector<u3dg_image> views(m_images.size());
+        for (std::size_t k = 0; k < m_images.size(); ++k)
+            views[k] = {m_images[k].camera, m_images[k].rgb.data()};
+        const u3dg_model v = initial.view();
+        check(u3dg_trainer_create(&v, views.data(), int(views.size()), sceneExtent, &m_options, &m_t));
+    }
+
+    ~Trainer() { u3dg_trainer_destroy(m_t); }
+    Trainer(const Trainer &) = delete;
+    Trainer &operator=(const Trainer &) = delete;
+
+    void step() { check(u3dg_trainer_step(m_t, 1)); }
+    bool done() const
+    {
+        int d = 0;
+        check(u3dg_trainer_done(m_t, &d));
+        return d != 0;
+    }
+    int iteration() const
+    {
+        int it = 0;
+        check(u3dg_trainer_iteration(m_t, &it));
+        return it;
+    }
+    // The current model, copied back from the GPU; valid until the next step().
+    const GaussianModel &model() const
+    {
+        std::size_t n = 0;
+        check(u3dg_trainer_size(m_t, &n));
+        m_model.resize(n);
+        u3dg_model v = m_model.view();
+        check(u3dg_trainer_download(m_t, &v, n, &n));
+        return m_model;
+    }
+    const TrainStats &stats() const
+    {
+        u3dg_train_stats s{};
+        check(u3dg_trainer_stats(m_t, &s));
+        m_stats.iteration = s.iteration;
+        m_stats.loss = s.loss;
+        m_stats.psnr = s.psnr;
+        m_stats.gaussians = std::size_t(s.gaussians);
+        return m_stats;
+    }
+    const std::vector<TrainImage> &images() const { return m_images; }
+    float evaluatePsnr()
+    {
+        float p = 0;
+        check(u3dg_trainer_eval_psnr(m_t, &p));
+        return p;
+    }
+    template <class Cam>
+    void render(const Cam &camera, std::vector<float> &rgb)
+    {
+        const RenderCamera c = cameraFrom(camera);
+        rgb.resize(std::size_t(c.width) * c.height * 3);
+        check(u3dg_trainer_render(m_t, &c, rgb.data()));
+    }
+
+private:
+    template <class Image>
+    static std::vector<TrainImage> convert(const std::vector<Image> &images)
+    {
+        std::vector<TrainImage> out;
+        out.reserve(images.size());
+        for (const Image &i : images)
+            out.push_back(imageFrom(i));
+        return out;
+    }
+
+    u3dg_trainer *m_t = nullptr;
+    std::vector<TrainImage> m_images;
+    TrainOptions m_options;
+    mutable GaussianModel m_model;
+    mutable TrainStats m_stats;
+};
+
+// ------------------------------------------------------------------ free functions
+
+// initGaussiansFromPoints (GaussianModel.h:41).
+inline GaussianModel initGaussiansFromPoints(const std::vector<float> &xyz, const std::vector<float> &rgb)
+{
+    GaussianModel m;
+    const std::size_t n = xyz.size() / 3;
+    m.resize(n);
+    u3dg_model v = m.view();
+    check(u3dg_init_gaussians_from_points(xyz.data(), rgb.size() >= n * 3 ? rgb.data() : nullptr, n, &v));
+    return m;
+}
+
+// writeSplatPly / readSplatPly (SplatPly.h:12-18): bool results and an optional error string.
+inline bool writeSplatPly(const std::string &path, const GaussianModel &model, std::string *error = nullptr)
+{
+    const u3dg_model v = model.view();
+    if (u3dg_write_splat_ply(path.c_str(), &v) == U3DG_OK)
+        return true;
+    if (error)
+        *error = u3dg_last_error();
+    return false;
+}
+
+inline bool readSplatPly(const std::string &path, GaussianModel &model, std::string *error = nullptr,
+                         bool *isSplat = nullptr)
+{
+    std::size_t n = 0;
+    int splat = 0;
+    if (u3dg_read_splat_ply(path.c_str(), nullptr, 0, &n, &splat) != U3DG_OK) {
+        if (error)
+            *error = u3dg_last_error();
+        return false;
+    }
+    model.resize(n);
+    u3dg_model v = model.view();
+    if (u3dg_read_splat_ply(path.c_str(), &v, n, &n, &splat) != U3DG_OK) {
+        if (error)
+            *error = u3dg_last_error();
+        return false;
+    }
+    if (isSplat)
+        *isSplat = splat != 0;
+    return true;
+}
+
+// photometricLoss / psnr (Loss.h:18-21).
+struct LossValue {
+    float total = 0, l1 = 0, ssim = 0;
+};
+
+inline LossValue photometricLoss(const float *render, const float *target, int width, int height, float ssimLambda,
+                                 float *grad)
+{
+    u3dg_loss_value v{};
+    check(u3dg_photometric_loss(render, target, width, height, ssimLambda, grad, &v));
+    return {v.total, v.l1, v.ssim};
+}
+
+inline float psnr(const float *a, const float *b, std::size_t count)
+{
+    float p = 0;
+    check(u3dg_psnr(a, b, count, &p));
+    return p;
+}
+
+} // namespace gpu
+} // namespace u3d

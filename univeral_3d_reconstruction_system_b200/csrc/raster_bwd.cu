@@ -1,0 +1,254 @@
+// raster_bwd.cu - tile compositing backward (Rasterizer::backward pass 1, Rasterizer.cpp:353-427).
+//
+// Same CTA / warp / batch layout as the forward (raster_common.cuh). Each pixel walks its tile list
+// back to front from its contributor count with the reference's recurrence (transmittance recovered
+// by division, running colour accumulation, clamp handling). A thread holds two pixels and adds their
+// contributions before the warp sum, so one warp reduction covers 64 pixels. The 9 sums per list entry
+// (dmean2d xy, dconic ABC, drgb, dalpha) go through a reduce-scatter (14 shuffles), land in a
+// per-warp shared-memory slot, and are added over the warps in warp order after the batch: the result
+// does not depend on scheduling. Each (tile, Gaussian) partial is stored once at the entry's emission
+// index, zero for entries behind every pixel's last contributor; the chain-rule kernel sums a
+// Gaussian's partials in tile order.
+//
+// Contribution decisions (power, alpha, the cut-offs) and the transmittance recovery are computed with
+// explicitly unfused operations, exactly as in the forward; the gradient arithmetic may use fused
+// multiply-add (gradients are compared within a relative tolerance).
+
+#include "raster_common.cuh"
+
+#include <atomic>
+
+namespace u3dg {
+
+namespace {
+
+struct PixelState {
+    float T, acc0, acc1, acc2, lc0, lc1, lc2, lastAlpha;
+    float fT, d0, d1, d2, bgDot, fy;
+    int nC;
+};
+
+// One back-to-front step of Rasterizer.cpp:385-416 for one pixel; adds its 9 contributions to c.
+__device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const float4 *sR, int jj, float dx,
+                                         float minA, PixelState &s, float c[kG2d])
+{
+    const float dy = __fsub_rn(P.y, s.fy);
+    const float power = powerAt(Q, dx, dy);
+    if (power > 0.0f)
+        return false;
+    const float G = rasterExp(power);
+    const float raw = __fmul_rn(Q.w, G);
+    const float al = (raw < kMaxAlpha) ? raw : kMaxAlpha;
+    if (al < minA)
+        return false;
+    const float4 R = sR[jj];
+    s.T = __fdiv_rn(s.T, __fsub_rn(1.0f, al));
+    const float w = al * s.T;
+    float dAl = 0.0f;
+    s.acc0 = s.lastAlpha * s.lc0 + (1.0f - s.lastAlpha) * s.acc0;
+    s.lc0 = R.x;
+    dAl += (R.x - s.acc0) * s.d0;
+    c[5] += w * s.d0;
+    s.acc1 = s.lastAlpha * s.lc1 + (1.0f - s.lastAlpha) * s.acc1;
+    s.lc1 = R.y;
+    dAl += (R.y - s.acc1) * s.d1;
+    c[6] += w * s.d1;
+    s.acc2 = s.lastAlpha * s.lc2 + (1.0f - s.lastAlpha) * s.acc2;
+    s.lc2 = R.z;
+    dAl += (R.z - s.acc2) * s.d2;
+    c[7] += w * s.d2;
+    dAl *= s.T;
+    s.lastAlpha = al;
+    // -finalT / (1 - alpha) * bgDot adds a signed zero when bgDot is 0 (black background), which leaves
+    // dAl unchanged: skip the division then.
+    if (s.bgDot != 0.0f)
+        dAl += -s.fT / (1.0f - al) * s.bgDot;
+    if (raw > kMaxAlpha)
+        return true; // clamped alpha: colour gradient only
+    c[8] += G * dAl;
+    const float dPow = Q.w * dAl * G;
+    c[0] += dPow * -(Q.x * dx + Q.y * dy);
+    c[1] += dPow * -(Q.z * dy + Q.y * dx);
+    c[2] += dPow * -0.5f * dx * dx;
+    c[3] += dPow * -dx * dy;
+    c[4] += dPow * -0.5f * dy * dy;
+    return true;
+}
+
+// Sum of c[0..8] over the warp: values 0..7 by reduce-scatter (xor 16/8/4 exchanges halve the
+// values a lane holds; xor 2/1 finish), value 8 by a butterfly. Lane 4v gets value v, every lane v8.
+__device__ __forceinline__ float warpReduce9(const float c[kG2d], int lane, float *v8)
+{
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    float w4[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float send = b4 ? c[i] : c[i + 4];
+        const float keep = b4 ? c[i + 4] : c[i];
+        w4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    float w2[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const float send = b3 ? w4[i] : w4[i + 2];
+        const float keep = b3 ? w4[i + 2] : w4[i];
+        w2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    float v;
+    {
+        const float send = b2 ? w2[0] : w2[1];
+        const float keep = b2 ? w2[1] : w2[0];
+        v = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    float e = c[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+    *v8 = e;
+    return v;
+}
+
+__device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix, float fy, const float *dLdRgb,
+                                          const float *finalT, const int *nContrib, const float *bg)
+{
+    s.nC = inside ? nContrib[pix] : 0;
+    s.fT = inside ? finalT[pix] : 0.0f;
+    s.d0 = inside ? dLdRgb[pix * 3] : 0.0f;
+    s.d1 = inside ? dLdRgb[pix * 3 + 1] : 0.0f;
+    s.d2 = inside ? dLdRgb[pix * 3 + 2] : 0.0f;
+    s.bgDot = bg[0] * s.d0 + bg[1] * s.d1 + bg[2] * s.d2;
+    s.T = s.fT;
+    s.acc0 = s.acc1 = s.acc2 = s.lc0 = s.lc1 = s.lc2 = s.lastAlpha = 0.0f;
+    s.fy = fy;
+}
+
+template <int PB>
+__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
+                                                                              const float *finalTIn,
+                                                                              const int *nContribIn, float *partial,
+                                                                              int useAtomics)
+{
+    using S = RasterShape<PB>;
+    constexpr int NT = S::NT, NW = S::NW;
+    __shared__ float4 sP[NT];
+    __shared__ float4 sQ[NT];
+    __shared__ float4 sR[NT];
+    __shared__ uint32_t mask[NW][NW];
+    __shared__ int sMax;
+    extern __shared__ float sWarp[]; // NW slots of NT entries x 9 sums
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const WarpBlock<PB> wb(warp, lane);
+    const int tile = tileOf<PB>(a);
+    const int start = a.tileOffsets[tile], end = a.tileOffsets[tile + 1];
+    const bool in0 = wb.px < a.width && wb.py0 < a.height, in1 = wb.px < a.width && wb.py1 < a.height;
+    PixelState s0, s1;
+    initPixel(s0, in0, in0 ? size_t(wb.py0) * a.width + wb.px : 0, float(wb.py0), dLdRgb, finalTIn, nContribIn, a.bg);
+    initPixel(s1, in1, in1 ? size_t(wb.py1) * a.width + wb.px : 0, float(wb.py1), dLdRgb, finalTIn, nContribIn, a.bg);
+    const float fx = float(wb.px);
+    const float minA = a.minAlpha;
+    const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
+    const int vIdx = (lane >> 2) & 7; // value held after warpReduce9 (lanes 4v)
+    if (tid == 0)
+        sMax = 0;
+    __syncthreads();
+    const int nMax = max(s0.nC, s1.nC);
+    if (nMax > 0)
+        atomicMax(&sMax, nMax);
+    __syncthreads();
+    const int jmax = sMax;
+    // Entries behind every pixel's last contributor get no gradient (the reference's per-tile
+    // accumulators start at zero); their partials are still written, as the chain-rule kernel sums
+    // every intersection of a Gaussian.
+    if (!useAtomics)
+        for (int j = jmax + tid; j < end - start; j += NT) {
+            float *dst = partial + size_t(a.listEmit[start + j]) * kG2d;
+#pragma unroll
+            for (int k = 0; k < kG2d; ++k)
+                dst[k] = 0.0f;
+        }
+    float *myWarp = sWarp + size_t(warp) * NT * kG2d;
+    for (int bEnd = jmax; bEnd > 0; bEnd -= NT) {
+        const int bStart = max(0, bEnd - NT), cnt = bEnd - bStart;
+        __syncthreads();
+        stage<PB>(rec, a.list, start + bStart + tid, tid < cnt, tid, sP, sQ, sR, mask);
+        {
+            float4 *z = reinterpret_cast<float4 *>(sWarp);
+            for (int k = tid; k < NW * NT * kG2d / 4; k += NT)
+                z[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        __syncthreads();
+        for (int k = NW - 1; k >= 0; --k) {
+            uint32_t bits = mask[warp][k];
+            while (bits) {
+                const int hb = 31 - __clz(bits);
+                bits &= ~(1u << hb);
+                const int jj = 32 * k + hb;
+                const int j = bStart + jj;
+                float c[kG2d];
+#pragma unroll
+                for (int q = 0; q < kG2d; ++q)
+                    c[q] = 0.0f;
+                bool act = false;
+                if (j < s0.nC || j < s1.nC) {
+                    const float4 P = sP[jj], Q = sQ[jj];
+                    const float dx = __fsub_rn(P.x, fx);
+                    if (j < s0.nC)
+                        act |= pairGrad(P, Q, sR, jj, dx, minA, s0, c);
+                    if (j < s1.nC)
+                        act |= pairGrad(P, Q, sR, jj, dx, minA, s1, c);
+                }
+                if (__any_sync(0xffffffffu, act)) {
+                    float v8;
+                    const float v = warpReduce9(c, lane, &v8);
+                    if ((lane & 3) == 0)
+                        myWarp[jj * kG2d + vIdx] = v;
+                    if (lane == 1)
+                        myWarp[jj * kG2d + 8] = v8;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < cnt) {
+            float sum[kG2d];
+#pragma unroll
+            for (int q = 0; q < kG2d; ++q)
+                sum[q] = sWarp[tid * kG2d + q];
+            for (int w = 1; w < NW; ++w)
+#pragma unroll
+                for (int q = 0; q < kG2d; ++q)
+                    sum[q] += sWarp[(size_t(w) * NT + tid) * kG2d + q];
+            float *dst = partial + size_t(a.listEmit[start + bStart + tid]) * kG2d;
+            if (useAtomics) {
+#pragma unroll
+                for (int q = 0; q < kG2d; ++q)
+                    atomicAdd(dst + q, sum[q]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < kG2d; ++q)
+                    dst[q] = sum[q];
+            }
+        }
+    }
+}
+
+} // namespace
+
+void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
+                             float *partial, cudaStream_t s)
+{
+    if (a.tileSize <= 8) {
+        dim3 g((a.width + 7) / 8, (a.height + 7) / 8);
+        constexpr int NT = RasterShape<8>::NT, NW = RasterShape<8>::NW;
+        const size_t smem = size_t(NW) * NT * kG2d * sizeof(float);
+        { compositeBackwardKernel<8><<<g, NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, 0); countLaunch(); }
+    } else {
+        dim3 g((a.width + 15) / 16, (a.height + 15) / 16);
+        constexpr int NT = RasterShape<16>::NT, NW = RasterShape<16>::NW;
+        const size_t smem = size_t(NW) * NT * kG2d * sizeof(float); // 18 KB: no opt-in needed
+        { compositeBackwardKernel<16><<<g, NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, a.tileSize > 16 ? 1 : 0); countLaunch(); }
+    }
+}
+
+} // namespace u3dg

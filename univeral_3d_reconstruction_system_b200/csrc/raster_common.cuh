@@ -1,0 +1,87 @@
+// raster_common.cuh - pixel layout and batch staging shared by the compositing kernels.
+//
+// A CTA covers a PB x PB pixel block (PB = 16, or 8 for tile size 8) with PB*PB/2 threads; a warp
+// owns an 8 x 8 pixel block and each thread two pixels of the same column, rows r and r + 4. A tile's
+// depth-sorted list is walked in batches of one record per thread; while staging a batch, warp k votes
+// which of its 32 entries meet each warp's pixel block (the Gaussian's conservative contributing box,
+// SplatRec::ex / ey, against the block), so each warp later walks only the set bits of its mask.
+#pragma once
+
+#include "kernels.h"
+
+namespace u3dg {
+
+template <int PB>
+struct RasterShape {
+    static constexpr int NT = PB * PB / 2; // threads = batch entries
+    static constexpr int NW = NT / 32;     // warps
+    static constexpr int WX = PB / 8;      // warp blocks per row
+};
+
+// This thread's two pixels and its warp's 8x8 block.
+template <int PB>
+struct WarpBlock {
+    int px, py0, py1;
+    float x0, x1, y0, y1; // warp block, inclusive
+    __device__ WarpBlock(int warp, int lane)
+    {
+        constexpr int WX = RasterShape<PB>::WX;
+        const int wx0 = int(blockIdx.x) * PB + (warp % WX) * 8, wy0 = int(blockIdx.y) * PB + (warp / WX) * 8;
+        px = wx0 + (lane & 7);
+        py0 = wy0 + (lane >> 3);
+        py1 = py0 + 4;
+        x0 = float(wx0);
+        x1 = float(wx0 + 7);
+        y0 = float(wy0);
+        y1 = float(wy0 + 7);
+    }
+};
+
+template <int PB>
+__device__ __forceinline__ bool meets(const float4 &p, int w)
+{
+    constexpr int WX = RasterShape<PB>::WX;
+    const float x0 = float(int(blockIdx.x) * PB + (w % WX) * 8), y0 = float(int(blockIdx.y) * PB + (w / WX) * 8);
+    return !(p.x + p.z < x0 || p.x - p.z > x0 + 7.0f || p.y + p.w < y0 || p.y - p.w > y0 + 7.0f);
+}
+
+template <int PB>
+__device__ __forceinline__ int tileOf(const RasterArgs &a)
+{
+    return (int(blockIdx.y) * PB / a.tileSize) * a.tilesX + int(blockIdx.x) * PB / a.tileSize;
+}
+
+// Stages batch entry `slot` (if valid) and the masks: mask[w][k] bit b <=> entry 32k + b meets warp w.
+template <int PB>
+__device__ __forceinline__ void stage(const float4 *rec, const int *list, int idx, bool valid, int slot, float4 *sP,
+                                      float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB>::NW])
+{
+    constexpr int NW = RasterShape<PB>::NW;
+    float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f);
+    if (valid) {
+        const float4 *r = rec + size_t(list[idx]) * 3;
+        p = r[0];
+        sP[slot] = p;
+        sQ[slot] = r[1];
+        sR[slot] = r[2];
+    }
+    const int warp = slot >> 5, lane = slot & 31;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t bits = __ballot_sync(0xffffffffu, valid && meets<PB>(p, w));
+        if (lane == 0)
+            mask[w][warp] = bits;
+    }
+}
+
+// Gaussian falloff exponent at one pixel, in the reference's operation order with no fused
+// multiply-add (Rasterizer.cpp:305-306), so every kernel decides contributions identically.
+__device__ __forceinline__ float powerAt(const float4 &Q, float dx, float dy)
+{
+    const float q = __fadd_rn(__fmul_rn(__fmul_rn(Q.x, dx), dx), __fmul_rn(__fmul_rn(Q.z, dy), dy));
+    return __fsub_rn(__fmul_rn(-0.5f, q), __fmul_rn(__fmul_rn(Q.y, dx), dy));
+}
+
+__device__ __forceinline__ float rasterExp(float x) { return expf(x); }
+
+} // namespace u3dg
