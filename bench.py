@@ -285,7 +285,30 @@ def run_ours(args, dist: Dist) -> dict:
         "workload_stats": {"gaussians": int(n), "intersections_per_step": int(i_avg), "pixels": int(p),
                            "loss_ema": stats.loss, "psnr_ema": stats.psnr, "e2e_psnr_ema": st2.psnr},
     }
+    if args.schedule:
+        res["schedule"] = run_full_schedule(args, sc)
     return res
+
+
+def run_full_schedule(args, sc) -> dict:
+    """The preset's whole schedule from its sparse initialisation (High: 30k noisy points,
+    TrainOptions::forIterations(7000), densification up to 300k): device training time, iterations/s over
+    the schedule, and the PSNR trajectory (evaluatePsnr after every 500 iterations, not timed)."""
+    from univeral_3d_reconstruction_system_b200 import api
+    from univeral_3d_reconstruction_system_b200.schedule import run_schedule
+
+    opt = sc.options()
+    init = api.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb)
+    t = api.Trainer(init, sc.images, sc.extent, opt)
+    r = run_schedule(t, opt.iterations, chunk=500)
+    out = r.as_dict()
+    out.update({"init": f"{init.size()} noisy points (initGaussiansFromPoints)",
+                "schedule": f"forIterations({opt.iterations}), max {opt.max_gaussians}",
+                "it_per_s": round(opt.iterations / max(r.total_seconds, 1e-9), 2),
+                "time_to_final_psnr_s": round(r.total_seconds, 4), "replays": t.replays()})
+    log(f"schedule: {opt.iterations} iterations in {r.total_seconds:.2f} s, PSNR {r.initial_psnr:.2f} -> "
+        f"{r.final_psnr:.2f} dB, {r.gaussians[-1] if r.gaussians else 0} Gaussians")
+    return out
 
 
 def cpu_baseline(args, seconds: float = 15.0) -> dict:
@@ -364,6 +387,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="high-300k")
+    ap.add_argument("--no-schedule", dest="schedule", action="store_false",
+                    help="skip the full-schedule run (PSNR trajectory, time to PSNR)")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling run for ncu: warm up, log the launch count, run this many steps, exit")
     args = ap.parse_args()
@@ -384,6 +409,8 @@ def main():
                 "config": config(args, dist), "roofline": res["roofline"], "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "phase_ms": res["phase_ms"],
                 "workload_stats": res["workload_stats"]}
+        if "schedule" in res:
+            line["schedule"] = res["schedule"]
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
         if dist.rank == 0:

@@ -304,6 +304,53 @@ int u3dg_render_sh(const u3dg_model *model, const float *sh_rest, int degree, co
 int u3dg_render_views_sh(const u3dg_model *model, const float *sh_rest, int degree, const u3dg_camera *cameras,
                          int count, const u3dg_raster_settings *settings, uint8_t *rgb8);
 
+/* ------------------------------------------------------------------ learned warm-start */
+
+/* No reference counterpart: the reference initialises with initGaussiansFromPoints
+ * (engine/src/splat/GaussianModel.cpp:68-144), which stays the fallback and the judge. A small FP32 MLP
+ * (134 -> 128 -> 128 -> 128 -> 11, ReLU) maps each SfM point's neighbourhood feature to its initial
+ * Gaussian: residual log-scales and DC colour over the plain initialisation, quaternion and logit
+ * opacity. Features (134 floats per point): 16 nearest points' relative positions (divided by the
+ * plain-init scale, 48) and log distances (16), their colours (48), colour samples minus 0.5 from the 7
+ * nearest views that see the point (21), and the fraction of those views found (1). Training, inference
+ * and gradients run on the GPU. */
+#define U3DG_MLP_INPUTS 134
+#define U3DG_MLP_OUTPUTS 11
+#define U3DG_MLP_PARAMS 51723
+
+typedef struct u3dg_mlp u3dg_mlp;
+
+/* Number of parameters (U3DG_MLP_PARAMS): per layer W (out x in, row-major) then b. */
+int u3dg_mlp_param_count(void);
+/* params (U3DG_MLP_PARAMS floats) or NULL for a seeded He-uniform initialisation whose output layer
+ * starts at the plain initialisation. */
+int u3dg_mlp_create(const float *params, unsigned int seed, u3dg_mlp **out);
+int u3dg_mlp_params(u3dg_mlp *mlp, float *out);
+/* y (n x 11) = network(x (n x 134)). */
+int u3dg_mlp_forward(u3dg_mlp *mlp, const float *x, size_t n, float *y);
+/* Weighted mean squared error against t (n x 11) with per-output weights (11, NULL = defaults), and
+ * its gradient with respect to every parameter (grad: U3DG_MLP_PARAMS floats, may be NULL). */
+int u3dg_mlp_loss_grad(u3dg_mlp *mlp, const float *x, const float *t, const float *weights, size_t n, float *loss,
+                       float *grad);
+/* Adam (lr, beta 0.9 / 0.999, eps 1e-8) over `epochs` shuffled passes (std::mt19937(seed)) of whole
+ * batches; epoch_loss (epochs floats, may be NULL) gets each epoch's mean batch loss. */
+int u3dg_mlp_train(u3dg_mlp *mlp, const float *x, const float *t, const float *weights, size_t n, int epochs,
+                   int batch, float lr, unsigned int seed, float *epoch_loss);
+void u3dg_mlp_destroy(u3dg_mlp *mlp);
+
+/* The k (1, 3 or 16) nearest points of every query (brute force on the GPU; ties by lower index);
+ * idx / dist2 get nq * k entries (-1 / FLT_MAX when fewer points exist). exclude_self skips the point
+ * whose index equals the query's. */
+int u3dg_knn(const float *queries, size_t nq, const float *points, size_t np, int k, int exclude_self, int *idx,
+             float *dist2);
+/* The 134-float feature of every point (features: n x 134). */
+int u3dg_warmstart_features(const float *xyz, const float *rgb, size_t n, const u3dg_image *images, int count,
+                            float *features);
+/* Initial model of n points through the network (out: n Gaussians); mlp == NULL gives exactly
+ * initGaussiansFromPoints. A point whose prediction is not finite keeps its plain initialisation. */
+int u3dg_warmstart_init(u3dg_mlp *mlp, const float *xyz, const float *rgb, size_t n, const u3dg_image *images,
+                        int count, u3dg_model *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,16 @@ SIGNATURES = {
     "u3dg_read_splat_ply": (C.c_int, [C.c_char_p, _MV, C.c_size_t, _SZ, _I]),
     "u3dg_render_sh": (C.c_int, [_MV, _F, C.c_int, _CAM, _ST, _F]),
     "u3dg_render_views_sh": (C.c_int, [_MV, _F, C.c_int, _CAM, C.c_int, _ST, _abi.u8p]),
+    "u3dg_mlp_param_count": (C.c_int, []),
+    "u3dg_mlp_create": (C.c_int, [_F, C.c_uint, _PP]),
+    "u3dg_mlp_params": (C.c_int, [_P, _F]),
+    "u3dg_mlp_forward": (C.c_int, [_P, _F, C.c_size_t, _F]),
+    "u3dg_mlp_loss_grad": (C.c_int, [_P, _F, _F, _F, C.c_size_t, _F, _F]),
+    "u3dg_mlp_train": (C.c_int, [_P, _F, _F, _F, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_uint, _F]),
+    "u3dg_mlp_destroy": (None, [_P]),
+    "u3dg_knn": (C.c_int, [_F, C.c_size_t, _F, C.c_size_t, C.c_int, C.c_int, _I, _F]),
+    "u3dg_warmstart_features": (C.c_int, [_F, _F, C.c_size_t, C.POINTER(_abi.Image), C.c_int, _F]),
+    "u3dg_warmstart_init": (C.c_int, [_P, _F, _F, C.c_size_t, C.POINTER(_abi.Image), C.c_int, _MV]),
 }
 
 _lib = None

@@ -377,5 +377,92 @@ def renderViewsSh(model: GaussianModel, sh_rest: np.ndarray | None, degree: int,
     return res
 
 
+MLP_INPUTS, MLP_OUTPUTS, MLP_PARAMS = 134, 11, 51723
+
+
+class WarmStartNet:
+    """The learned warm-start MLP (134 -> 128 -> 128 -> 128 -> 11, FP32) on the GPU."""
+
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0):
+        h = C.c_void_p()
+        p = None
+        if params is not None:
+            params = np.ascontiguousarray(params, np.float32).reshape(-1)
+            if params.size != MLP_PARAMS:
+                raise ValueError(f"expected {MLP_PARAMS} parameters, got {params.size}")
+            p = _abi.fptr(params)
+        check(load().u3dg_mlp_create(p, seed, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            load().u3dg_mlp_destroy(h)
+            self._h = None
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, np.float32)
+        check(load().u3dg_mlp_params(self._h, _abi.fptr(out)))
+        return out
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_INPUTS)
+        y = np.zeros((x.shape[0], MLP_OUTPUTS), np.float32)
+        check(load().u3dg_mlp_forward(self._h, _abi.fptr(x), x.shape[0], _abi.fptr(y)))
+        return y
+
+    def loss_grad(self, x, t, weights=None):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_INPUTS)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, MLP_OUTPUTS)
+        w = _abi.fptr(np.ascontiguousarray(weights, np.float32)) if weights is not None else None
+        loss = C.c_float()
+        grad = np.zeros(MLP_PARAMS, np.float32)
+        check(load().u3dg_mlp_loss_grad(self._h, _abi.fptr(x), _abi.fptr(t), w, x.shape[0], C.byref(loss),
+                                        _abi.fptr(grad)))
+        return float(loss.value), grad
+
+    def train(self, x, t, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0, weights=None):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_INPUTS)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, MLP_OUTPUTS)
+        w = _abi.fptr(np.ascontiguousarray(weights, np.float32)) if weights is not None else None
+        losses = np.zeros(max(epochs, 1), np.float32)
+        check(load().u3dg_mlp_train(self._h, _abi.fptr(x), _abi.fptr(t), w, x.shape[0], epochs, batch, lr, seed,
+                                    _abi.fptr(losses)))
+        return losses[:epochs]
+
+
+def knn(queries: np.ndarray, points: np.ndarray, k: int, exclude_self: bool = False):
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 3)
+    p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    idx = np.zeros((q.shape[0], k), np.int32)
+    d2 = np.zeros((q.shape[0], k), np.float32)
+    check(load().u3dg_knn(_abi.fptr(q), q.shape[0], _abi.fptr(p), p.shape[0], k, int(exclude_self),
+                          _abi.iptr(idx), _abi.fptr(d2)))
+    return idx, d2
+
+
+def warmstartFeatures(xyz, rgb, images) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    rgbp = _abi.fptr(np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)) if rgb is not None else None
+    arr, keep = images_struct(images)
+    f = np.zeros((xyz.shape[0], MLP_INPUTS), np.float32)
+    check(load().u3dg_warmstart_features(_abi.fptr(xyz), rgbp, xyz.shape[0], arr, len(images), _abi.fptr(f)))
+    del keep
+    return f
+
+
+def warmstartInit(net: WarmStartNet | None, xyz, rgb, images) -> GaussianModel:
+    """Initial model through the network; net=None gives initGaussiansFromPoints exactly."""
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    rgbp = _abi.fptr(np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)) if rgb is not None else None
+    arr, keep = images_struct(images)
+    out = GaussianModel.zeros(xyz.shape[0])
+    v = out.view()
+    check(load().u3dg_warmstart_init(net._h if net is not None else None, _abi.fptr(xyz), rgbp, xyz.shape[0], arr,
+                                     len(images), C.byref(v)))
+    del keep
+    return out
+
+
 __all__ = ["Trainer", "Rasterizer", "binTiles", "photometricLoss", "psnr", "Adam", "densifyAndPrune",
            "initGaussiansFromPoints", "writeSplatPly", "readSplatPly", "renderSh", "U3dgError", "TrainImage"]

@@ -12,32 +12,10 @@ using namespace u3dg;
 
 namespace {
 
-thread_local std::string tLastError;
-
-int setError(int code, const std::string &msg)
-{
-    tLastError = msg;
-    return code;
-}
-
 template <class F>
 int guarded(F &&f)
 {
-    try {
-        f();
-        return U3DG_OK;
-    } catch (const StatusError &e) {
-        return setError(e.status, e.what());
-    } catch (const CudaError &e) {
-        const int code = (e.code == cudaErrorMemoryAllocation) ? U3DG_ERR_OOM
-                         : (e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver) ? U3DG_ERR_NO_DEVICE
-                                                                                                   : U3DG_ERR_CUDA;
-        return setError(code, e.what());
-    } catch (const std::bad_alloc &) {
-        return setError(U3DG_ERR_OOM, "host allocation failed");
-    } catch (const std::exception &e) {
-        return setError(U3DG_ERR_STATE, e.what());
-    }
+    return guardedCall(std::forward<F>(f));
 }
 
 void requireDevice()
@@ -130,7 +108,7 @@ struct u3dg_adam {
 
 extern "C" {
 
-const char *u3dg_last_error(void) { return tLastError.c_str(); }
+const char *u3dg_last_error(void) { return lastError(); }
 
 int u3dg_abi_version(void) { return U3DG_ABI_VERSION; }
 

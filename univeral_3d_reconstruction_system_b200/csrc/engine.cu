@@ -26,6 +26,16 @@ void countLaunch() { gLaunches.fetch_add(1, std::memory_order_relaxed); }
 
 unsigned long long launchCount() { return gLaunches.load(std::memory_order_relaxed); }
 
+static thread_local std::string tLastError;
+
+int setError(int code, const std::string &msg)
+{
+    tLastError = msg;
+    return code;
+}
+
+const char *lastError() { return tLastError.c_str(); }
+
 void checkSettings(const u3dg_raster_settings &st)
 {
     if (!(st.tile_size == 8 || (st.tile_size >= 16 && st.tile_size % 16 == 0 && st.tile_size <= 256)))

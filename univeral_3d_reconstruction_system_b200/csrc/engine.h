@@ -26,6 +26,31 @@ struct StatusError : std::runtime_error {
     StatusError(int s, const std::string &m) : std::runtime_error(m), status(s) {}
 };
 
+// Thread-local message behind u3dg_last_error; returns `code`.
+int setError(int code, const std::string &msg);
+const char *lastError();
+
+// Runs f, turning every C++ exception into a status code and a message (the C ABI never throws).
+template <class F>
+int guardedCall(F &&f)
+{
+    try {
+        f();
+        return U3DG_OK;
+    } catch (const StatusError &e) {
+        return setError(e.status, e.what());
+    } catch (const CudaError &e) {
+        const int code = (e.code == cudaErrorMemoryAllocation) ? U3DG_ERR_OOM
+                         : (e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver) ? U3DG_ERR_NO_DEVICE
+                                                                                                   : U3DG_ERR_CUDA;
+        return setError(code, e.what());
+    } catch (const std::bad_alloc &) {
+        return setError(U3DG_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return setError(U3DG_ERR_STATE, e.what());
+    }
+}
+
 #define U3DG_CUDA(x)                                                   \
     do {                                                               \
         cudaError_t e_ = (x);                                          \

@@ -1,0 +1,430 @@
+// warmstart.cu - learned warm-start: neighbourhood features, a small FP32 MLP (forward, backward, Adam)
+// and its inference into an initial GaussianModel. No reference counterpart: the reference initialises
+// with initGaussiansFromPoints (GaussianModel.cpp:68-144), which stays the fallback and the judge.
+//
+// Features (134 floats per SfM point):
+//   [0, 48)    relative positions of the 16 nearest points, divided by the point's plain-init scale
+//   [48, 64)   natural log of the 16 neighbour distances
+//   [64, 112)  colours of the 16 nearest points
+//   [112, 133) colour samples (minus 0.5) from the 7 nearest views that see the point in their image
+//   133        number of those views / 7
+// Network: 134 -> 128 -> 128 -> 128 -> 11, ReLU between layers, FP32. Parameters in one flat vector,
+// per layer W (out x in, row-major) then b. All reductions run in a fixed order (deterministic).
+//
+// The work is tiny next to training (51.7k parameters); the kernels are plain SIMT FP32: tiled GEMMs
+// with shared-memory staging, brute-force tiled k-nearest-neighbour search.
+
+#include "kernels.h"
+#include "warmstart.h"
+
+#include <cfloat>
+
+namespace u3dg {
+
+namespace {
+
+inline int cdiv(long long a, int b) { return int((a + b - 1) / b); }
+
+// ------------------------------------------------------------------ k nearest neighbours
+
+// For every query, the K nearest points (squared distance, ties by lower index); candidates are
+// staged in shared memory 256 at a time. excludeSelf skips the point with the query's own index.
+template <int K>
+__global__ void __launch_bounds__(256) knnKernel(const float *queries, int nq, const float *points, int np,
+                                                 int excludeSelf, int *outIdx, float *outD2)
+{
+    __shared__ float sx[256], sy[256], sz[256];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    float qx = 0, qy = 0, qz = 0;
+    if (q < nq) {
+        qx = queries[3 * q];
+        qy = queries[3 * q + 1];
+        qz = queries[3 * q + 2];
+    }
+    float bd[K];
+    int bi[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        bd[k] = FLT_MAX;
+        bi[k] = -1;
+    }
+    for (int c0 = 0; c0 < np; c0 += 256) {
+        __syncthreads();
+        const int c = c0 + threadIdx.x;
+        if (c < np) {
+            sx[threadIdx.x] = points[3 * c];
+            sy[threadIdx.x] = points[3 * c + 1];
+            sz[threadIdx.x] = points[3 * c + 2];
+        }
+        __syncthreads();
+        const int cnt = min(256, np - c0);
+        if (q >= nq)
+            continue;
+        for (int j = 0; j < cnt; ++j) {
+            const int idx = c0 + j;
+            if (excludeSelf && idx == q)
+                continue;
+            const float dx = sx[j] - qx, dy = sy[j] - qy, dz = sz[j] - qz;
+            float d = dx * dx + dy * dy + dz * dz;
+            if (!(d < bd[K - 1]))
+                continue;
+            int id = idx;
+            // Insertion into the sorted list (strict <: an equal distance keeps the lower index first).
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (d < bd[k]) {
+                    const float td = bd[k];
+                    const int ti = bi[k];
+                    bd[k] = d;
+                    bi[k] = id;
+                    d = td;
+                    id = ti;
+                }
+            }
+        }
+    }
+    if (q < nq) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            outIdx[size_t(q) * K + k] = bi[k];
+            outD2[size_t(q) * K + k] = bd[k];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ features
+
+struct ViewRef {
+    u3dg_camera cam;
+    const uint8_t *rgb;
+    float cx, cy, cz; // camera centre
+};
+
+__global__ void __launch_bounds__(128) featuresKernel(const float *xyz, const float *rgb, int n, const int *nbr,
+                                                      const float *nd2, const float *baseScale,
+                                                      const ViewRef *views, int nViews, float *feat)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float *f = feat + size_t(i) * kWarmInputs;
+    const float px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
+    const float s = baseScale[i];
+    const float inv = s > 0.0f ? 1.0f / s : 0.0f;
+    for (int k = 0; k < kWarmNeighbours; ++k) {
+        const int j = nbr[size_t(i) * kWarmNeighbours + k];
+        if (j < 0) {
+            f[3 * k] = f[3 * k + 1] = f[3 * k + 2] = 0.0f;
+            f[48 + k] = 0.0f;
+            f[64 + 3 * k] = f[64 + 3 * k + 1] = f[64 + 3 * k + 2] = 0.0f;
+            continue;
+        }
+        f[3 * k] = (xyz[3 * j] - px) * inv;
+        f[3 * k + 1] = (xyz[3 * j + 1] - py) * inv;
+        f[3 * k + 2] = (xyz[3 * j + 2] - pz) * inv;
+        f[48 + k] = 0.5f * logf(fmaxf(nd2[size_t(i) * kWarmNeighbours + k], 1e-20f));
+        for (int c = 0; c < 3; ++c)
+            f[64 + 3 * k + c] = rgb ? rgb[3 * j + c] : 0.5f;
+    }
+    // The 7 nearest views (camera centre distance) in which the point lies in front and inside.
+    float bd[kWarmViews];
+    int bv[kWarmViews];
+    int bu[kWarmViews], bw[kWarmViews];
+    for (int k = 0; k < kWarmViews; ++k) {
+        bd[k] = FLT_MAX;
+        bv[k] = -1;
+        bu[k] = bw[k] = 0;
+    }
+    for (int v = 0; v < nViews; ++v) {
+        const ViewRef &vr = views[v];
+        const float *R = vr.cam.R;
+        const float x = R[0] * px + R[1] * py + R[2] * pz + vr.cam.t[0];
+        const float y = R[3] * px + R[4] * py + R[5] * pz + vr.cam.t[1];
+        const float z = R[6] * px + R[7] * py + R[8] * pz + vr.cam.t[2];
+        if (!(z > 1e-3f))
+            continue;
+        const int u = __float2int_rn(vr.cam.fx * x / z + vr.cam.cx);
+        const int w = __float2int_rn(vr.cam.fy * y / z + vr.cam.cy);
+        if (u < 0 || w < 0 || u >= vr.cam.width || w >= vr.cam.height)
+            continue;
+        const float dx = px - vr.cx, dy = py - vr.cy, dz = pz - vr.cz;
+        float d = dx * dx + dy * dy + dz * dz;
+        int vv = v, uu = u, ww = w;
+        for (int k = 0; k < kWarmViews; ++k) {
+            if (d < bd[k]) {
+                const float td = bd[k];
+                const int tv = bv[k], tu = bu[k], tw = bw[k];
+                bd[k] = d;
+                bv[k] = vv;
+                bu[k] = uu;
+                bw[k] = ww;
+                d = td;
+                vv = tv;
+                uu = tu;
+                ww = tw;
+            }
+        }
+    }
+    int seen = 0;
+    for (int k = 0; k < kWarmViews; ++k) {
+        float c3[3] = {0.0f, 0.0f, 0.0f};
+        if (bv[k] >= 0) {
+            const ViewRef &vr = views[bv[k]];
+            const uint8_t *px8 = vr.rgb + (size_t(bw[k]) * vr.cam.width + bu[k]) * 3;
+            for (int c = 0; c < 3; ++c)
+                c3[c] = float(px8[c]) * (1.0f / 255.0f) - 0.5f;
+            ++seen;
+        }
+        for (int c = 0; c < 3; ++c)
+            f[112 + 3 * k + c] = c3[c];
+    }
+    f[133] = float(seen) / float(kWarmViews);
+}
+
+// ------------------------------------------------------------------ GEMM for the MLP
+
+// C[m][n] (row-major, ldc) = sum_k A(m, k) B(k, n) (+ bias[n]) (ReLU), with A(m, k) = A[m*sAm + k*sAk]
+// and B(k, n) = B[k*sBk + n*sBn]. 64x64 output tile per CTA, k staged 16 at a time, 4x4 per thread.
+__global__ void __launch_bounds__(256) gemmKernel(const float *A, int sAm, int sAk, const float *B, int sBk, int sBn,
+                                                  float *C, int ldc, int M, int N, int K, const float *bias, int relu)
+{
+    __shared__ float As[16][64 + 1];
+    __shared__ float Bs[16][64 + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    float acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            acc[a][b] = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+            const int kk = e / 64, mm = e % 64;
+            const int m = m0 + mm, k = k0 + kk;
+            As[kk][mm] = (m < M && k < K) ? A[size_t(m) * sAm + size_t(k) * sAk] : 0.0f;
+            const int n = n0 + mm;
+            Bs[kk][mm] = (n < N && k < K) ? B[size_t(k) * sBk + size_t(n) * sBn] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                a[r] = As[kk][ty * 4 + r];
+                b[r] = Bs[kk][tx * 4 + r];
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    acc[r][c] += a[r] * b[c];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int m = m0 + ty * 4 + r;
+        if (m >= M)
+            continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int n = n0 + tx * 4 + c;
+            if (n >= N)
+                continue;
+            float v = acc[r][c];
+            if (bias)
+                v += bias[n];
+            if (relu)
+                v = v > 0.0f ? v : 0.0f;
+            C[size_t(m) * ldc + n] = v;
+        }
+    }
+}
+
+// dZ = dY where the layer's ReLU output was positive, else 0 (in place).
+__global__ void reluBackwardKernel(float *d, const float *y, size_t count)
+{
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < count && !(y[k] > 0.0f))
+        d[k] = 0.0f;
+}
+
+// db[o] = sum over the n rows of dZ[:, o], in row order.
+__global__ void columnSumKernel(const float *d, int n, int out, float *db)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= out)
+        return;
+    float s = 0.0f;
+    for (int r = 0; r < n; ++r)
+        s += d[size_t(r) * out + o];
+    db[o] = s;
+}
+
+// Weighted MSE: per block partial loss, and dY = 2 w (y - t) / (n * outputs).
+__global__ void __launch_bounds__(256) mseKernel(const float *y, const float *t, const float *w, int n, float *dy,
+                                                 double *partial)
+{
+    __shared__ double sh[256];
+    const size_t total = size_t(n) * kWarmOutputs;
+    const float scale = 2.0f / float(total);
+    double s = 0.0;
+    for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < total; k += size_t(gridDim.x) * blockDim.x) {
+        const int o = int(k % kWarmOutputs);
+        const float e = y[k] - t[k];
+        s += double(w[o]) * double(e) * double(e);
+        dy[k] = scale * w[o] * e;
+    }
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = sh[0];
+}
+
+__global__ void sumDoublesKernel(const double *p, int n, size_t count, float *out)
+{
+    double s = 0.0;
+    for (int k = 0; k < n; ++k)
+        s += p[k];
+    *out = float(s / double(count));
+}
+
+__global__ void adamFlatKernel(float *p, const float *g, float *m, float *v, int n, float stepSize, float invSqrtBc2,
+                               float eps)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const float gk = g[k];
+    const float mk = 0.9f * m[k] + 0.1f * gk;
+    const float vk = 0.999f * v[k] + 0.001f * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    p[k] -= stepSize * mk / (sqrtf(vk) * invSqrtBc2 + eps);
+}
+
+__global__ void gatherRowsKernel(const float *src, int width, const int *rows, int n, float *dst)
+{
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < size_t(n) * width) {
+        const size_t r = k / width, c = k % width;
+        dst[k] = src[size_t(rows[r]) * width + c];
+    }
+}
+
+// Initial model from the plain initialisation and the network's 11 outputs: log-scales and DC colour
+// as residuals over the plain values, quaternion and logit opacity directly. Non-finite outputs fall
+// back to the plain values for that Gaussian.
+__global__ void combineKernel(const float *pred, int n, float *scales, float *quats, float *opac, float *colors)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float *y = pred + size_t(i) * kWarmOutputs;
+    bool ok = true;
+    for (int k = 0; k < kWarmOutputs; ++k)
+        ok = ok && isfinite(y[k]);
+    if (!ok)
+        return;
+    for (int k = 0; k < 3; ++k) {
+        scales[3 * i + k] += y[k];
+        colors[3 * i + k] += y[8 + k];
+    }
+    for (int k = 0; k < 4; ++k)
+        quats[4 * i + k] = y[3 + k];
+    opac[i] = y[7];
+}
+
+} // namespace
+
+void launchKnn(const float *queries, int nq, const float *points, int np, int k, int excludeSelf, int *idx,
+               float *d2, cudaStream_t s)
+{
+    if (nq <= 0)
+        return;
+    if (k == 16) {
+        knnKernel<16><<<cdiv(nq, 256), 256, 0, s>>>(queries, nq, points, np, excludeSelf, idx, d2);
+    } else if (k == 3) {
+        knnKernel<3><<<cdiv(nq, 256), 256, 0, s>>>(queries, nq, points, np, excludeSelf, idx, d2);
+    } else {
+        knnKernel<1><<<cdiv(nq, 256), 256, 0, s>>>(queries, nq, points, np, excludeSelf, idx, d2);
+    }
+    countLaunch();
+}
+
+void launchWarmFeatures(const float *xyz, const float *rgb, int n, const int *nbr, const float *nd2,
+                        const float *baseScale, const void *views, int nViews, float *feat, cudaStream_t s)
+{
+    if (n > 0)
+        { featuresKernel<<<cdiv(n, 128), 128, 0, s>>>(xyz, rgb, n, nbr, nd2, baseScale, static_cast<const ViewRef *>(views), nViews, feat); countLaunch(); }
+}
+
+size_t warmViewRefBytes() { return sizeof(ViewRef); }
+
+void fillWarmViewRef(void *dst, const u3dg_camera &cam, const uint8_t *rgbDev)
+{
+    ViewRef v;
+    v.cam = cam;
+    v.rgb = rgbDev;
+    v.cx = -(cam.R[0] * cam.t[0] + cam.R[3] * cam.t[1] + cam.R[6] * cam.t[2]);
+    v.cy = -(cam.R[1] * cam.t[0] + cam.R[4] * cam.t[1] + cam.R[7] * cam.t[2]);
+    v.cz = -(cam.R[2] * cam.t[0] + cam.R[5] * cam.t[1] + cam.R[8] * cam.t[2]);
+    *static_cast<ViewRef *>(dst) = v;
+}
+
+void launchGemm(const float *A, int sAm, int sAk, const float *B, int sBk, int sBn, float *C, int ldc, int M, int N,
+                int K, const float *bias, bool relu, cudaStream_t s)
+{
+    if (M <= 0 || N <= 0)
+        return;
+    dim3 g(cdiv(N, 64), cdiv(M, 64));
+    { gemmKernel<<<g, 256, 0, s>>>(A, sAm, sAk, B, sBk, sBn, C, ldc, M, N, K, bias, relu ? 1 : 0); countLaunch(); }
+}
+
+void launchReluBackward(float *d, const float *y, size_t count, cudaStream_t s)
+{
+    if (count)
+        { reluBackwardKernel<<<cdiv((long long)count, 256), 256, 0, s>>>(d, y, count); countLaunch(); }
+}
+
+void launchColumnSum(const float *d, int n, int out, float *db, cudaStream_t s)
+{
+    { columnSumKernel<<<cdiv(out, 128), 128, 0, s>>>(d, n, out, db); countLaunch(); }
+}
+
+int mseBlocks() { return 148; }
+
+void launchMse(const float *y, const float *t, const float *w, int n, float *dy, double *partial, float *lossOut,
+               cudaStream_t s)
+{
+    { mseKernel<<<mseBlocks(), 256, 0, s>>>(y, t, w, n, dy, partial); countLaunch(); }
+    { sumDoublesKernel<<<1, 1, 0, s>>>(partial, mseBlocks(), size_t(n) * kWarmOutputs, lossOut); countLaunch(); }
+}
+
+void launchAdamFlat(float *p, const float *g, float *m, float *v, int n, float stepSize, float invSqrtBc2, float eps,
+                    cudaStream_t s)
+{
+    if (n > 0)
+        { adamFlatKernel<<<cdiv(n, 256), 256, 0, s>>>(p, g, m, v, n, stepSize, invSqrtBc2, eps); countLaunch(); }
+}
+
+void launchGatherRows(const float *src, int width, const int *rows, int n, float *dst, cudaStream_t s)
+{
+    if (n > 0)
+        { gatherRowsKernel<<<cdiv((long long)n * width, 256), 256, 0, s>>>(src, width, rows, n, dst); countLaunch(); }
+}
+
+void launchWarmCombine(const float *pred, int n, float *scales, float *quats, float *opac, float *colors, cudaStream_t s)
+{
+    if (n > 0)
+        { combineKernel<<<cdiv(n, 256), 256, 0, s>>>(pred, n, scales, quats, opac, colors); countLaunch(); }
+}
+
+} // namespace u3dg
