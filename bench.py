@@ -211,8 +211,11 @@ def run_ours(args, dist: Dist) -> dict:
         t.step(W)
         t.synchronize()
         log(f"launches_before={int(L.u3dg_launch_count())} launches_per_step_follow")
+        import torch  # NVTX range "steps" marks the captured training steps for ncu --nvtx-include steps/
+        torch.cuda.nvtx.range_push("steps")
         t.step(args.ncu_steps)
         t.synchronize()
+        torch.cuda.nvtx.range_pop()
         log(f"launches_after={int(L.u3dg_launch_count())}")
         return None
     total_needed = W + K + args.profile_steps
@@ -285,9 +288,38 @@ def run_ours(args, dist: Dist) -> dict:
         "workload_stats": {"gaussians": int(n), "intersections_per_step": int(i_avg), "pixels": int(p),
                            "loss_ema": stats.loss, "psnr_ema": stats.psnr, "e2e_psnr_ema": st2.psnr},
     }
+    it_s = res["value"]
+    res["workload_stats"].update({
+        "gaussians_pixels_per_s": n * p * it_s,
+        "pair_evaluations_per_s": i_avg * 256 * it_s,  # E = sum over tiles of pixels x list length (16x16)
+    })
     if args.schedule:
         res["schedule"] = run_full_schedule(args, sc)
+    if args.warmstart and dist.world == 1:
+        res["warmstart"] = run_warmstart(args)
     return res
+
+
+def run_warmstart(args) -> dict | None:
+    """Learned warm-start vs plain initialisation on one held-out High scene: both run the full
+    forIterations(7000) schedule; time-to-PSNR = initialisation wall time + device training time until
+    evaluatePsnr first reaches the plain run's final PSNR (evaluations every 250 iterations, not timed)."""
+    from univeral_3d_reconstruction_system_b200 import warmstart as ws
+
+    if not ws.WEIGHTS_PATH.exists():
+        return {"unavailable": f"{ws.WEIGHTS_PATH.name} not generated"}
+    params, meta = ws.load_params()
+    net = ws.api.WarmStartNet(params)
+    r = ws.evaluate_seed(net, ws.EVAL_SEEDS[0], chunk=250)
+    out = {k: r[k] for k in ("seed", "gt_count", "target_psnr", "plain_time_s", "warm_time_to_target_s",
+                             "time_ratio", "plain_final_psnr", "warm_final_psnr", "plain_initial_psnr",
+                             "warm_initial_psnr")}
+    out["network"] = f"{ws.WEIGHTS_PATH.name}: trained on {len(meta.get('train_seeds', []))} label scenes"
+    out["psnr_plain"] = r["plain"]["psnr"]
+    out["psnr_warm"] = r["warm"]["psnr"]
+    out["iterations"] = r["plain"]["iterations"]
+    log(f"warm-start: ratio {out['time_ratio']}, final {out['plain_final_psnr']} vs {out['warm_final_psnr']} dB")
+    return out
 
 
 def run_full_schedule(args, sc) -> dict:
@@ -389,6 +421,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="high-300k")
     ap.add_argument("--no-schedule", dest="schedule", action="store_false",
                     help="skip the full-schedule run (PSNR trajectory, time to PSNR)")
+    ap.add_argument("--no-warmstart", dest="warmstart", action="store_false",
+                    help="skip the learned warm-start vs plain comparison")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling run for ncu: warm up, log the launch count, run this many steps, exit")
     args = ap.parse_args()
@@ -409,8 +443,9 @@ def main():
                 "config": config(args, dist), "roofline": res["roofline"], "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "phase_ms": res["phase_ms"],
                 "workload_stats": res["workload_stats"]}
-        if "schedule" in res:
-            line["schedule"] = res["schedule"]
+        for key in ("schedule", "warmstart"):
+            if key in res:
+                line[key] = res[key]
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
         if dist.rank == 0:

@@ -1,0 +1,276 @@
+"""Learned warm-start: the CPU oracle of the network and kNN pinned by finite differences and brute
+force, the label canonical form, and (on the GPU) the CUDA kernels against the oracle, training,
+and the gain of the trained network over the plain initialisation."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import warmstart_oracle as wo
+from univeral_3d_reconstruction_system_b200 import warmstart as ws
+from univeral_3d_reconstruction_system_b200.types import GaussianModel
+
+from helpers import grad_close
+
+
+def _params(seed=0, scale=1.0):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(wo.PARAMS)
+    o = 0
+    for i, n in wo.LAYERS:
+        p[o:o + i * n] = rng.uniform(-1, 1, i * n) * np.sqrt(6.0 / i) * scale
+        o += i * n
+        p[o:o + n] = rng.normal(0, 0.1, n)
+        o += n
+    return p
+
+
+def _batch(n, seed=1):
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=(n, wo.INPUTS)), rng.normal(size=(n, wo.OUTPUTS))
+
+
+# ------------------------------------------------------------------ CPU: oracle and host logic
+
+
+def test_param_count_matches_header():
+    assert wo.PARAMS == 51723
+
+
+def test_oracle_mlp_gradient_matches_central_differences():
+    p = _params(3)
+    x, t = _batch(16)
+    w = np.linspace(0.25, 1.0, wo.OUTPUTS)
+    loss, g = wo.mlp_loss_grad(p, x, t, w)
+    rng = np.random.default_rng(5)
+    # Every layer's biases and a sample of weights.
+    picks = list(rng.choice(wo.PARAMS, 200, replace=False))
+    o = 0
+    for i, n in wo.LAYERS:
+        o += i * n
+        picks += list(range(o, o + min(n, 8)))
+        o += n
+    h = 1e-6
+    for k in picks:
+        pp, pm = p.copy(), p.copy()
+        pp[k] += h
+        pm[k] -= h
+        fd = (wo.mlp_loss(pp, x, t, w) - wo.mlp_loss(pm, x, t, w)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])) + 1e-8, (k, fd, g[k])
+    assert loss > 0
+
+
+def test_oracle_knn_matches_brute_force_with_ties():
+    rng = np.random.default_rng(2)
+    pts = rng.integers(-3, 4, size=(60, 3)).astype(np.float32) * 0.5  # lattice: many equal distances
+    idx, d2 = wo.knn(pts, pts, 16, exclude_self=True)
+    for i in range(len(pts)):
+        d = ((pts.astype(np.float64) - pts[i]) ** 2).sum(1)
+        d[i] = np.inf
+        order = sorted(range(len(pts)), key=lambda j: (d[j], j))[:16]
+        assert list(idx[i]) == order
+        np.testing.assert_array_equal(d2[i], d[order].astype(np.float32))
+
+
+def test_canonical_shape_preserves_covariance_and_is_canonical():
+    rng = np.random.default_rng(4)
+    n = 500
+    s = rng.normal(-3, 0.7, (n, 3))
+    q = rng.normal(size=(n, 4))
+    ss, qq = ws.canonical_shape(s, q)
+    assert np.all(np.diff(ss, axis=1) <= 0)
+    assert np.all(qq[:, 0] >= 0)
+    np.testing.assert_allclose(np.linalg.norm(qq, axis=1), 1.0, atol=1e-12)
+    R0, R1 = ws.quat_to_rot(q), ws.quat_to_rot(qq)
+    S0 = np.einsum("nij,nj,nkj->nik", R0, np.exp(2 * s), R0)
+    S1 = np.einsum("nij,nj,nkj->nik", R1, np.exp(2 * ss), R1)
+    np.testing.assert_allclose(S1, S0, rtol=1e-9, atol=1e-15)
+    # The same covariance from a different quaternion (sign flip, axis permutation) maps to one form.
+    perm = np.array([2, 0, 1])
+    Rp = R0[:, :, perm] * np.array([1, -1, -1])
+    if np.any(np.linalg.det(Rp) < 0):
+        Rp[:, :, 0] *= np.where(np.linalg.det(Rp) < 0, -1, 1)[:, None]
+    s2, q2 = ws.canonical_shape(s[:, perm], ws.rot_to_quat(Rp))
+    np.testing.assert_allclose(s2, ss, atol=1e-12)
+    np.testing.assert_allclose(q2, qq, atol=1e-9)
+
+
+def test_quaternion_round_trip():
+    rng = np.random.default_rng(8)
+    q = rng.normal(size=(300, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q *= np.where(q[:, :1] < 0, -1, 1)
+    np.testing.assert_allclose(ws.rot_to_quat(ws.quat_to_rot(q)), q, atol=1e-9)
+
+
+def test_folded_standardiser_equals_standardised_network():
+    p = _params(6).astype(np.float32)
+    rng = np.random.default_rng(9)
+    x = rng.normal(3.0, 5.0, size=(64, wo.INPUTS))
+    mu, sd = ws.standardiser(x)
+    y_std, _ = wo.mlp_forward(p, (x - mu) / sd)
+    y_fold, _ = wo.mlp_forward(ws.fold_standardiser(p, mu, sd), x)
+    np.testing.assert_allclose(y_fold, y_std, rtol=1e-4, atol=1e-4)
+
+
+def test_canonical_targets_of_the_plain_init_are_the_plain_outputs():
+    rng = np.random.default_rng(10)
+    n = 50
+    base = GaussianModel(rng.normal(size=(n, 3)), np.repeat(rng.normal(-3, .3, (n, 1)), 3, 1),
+                         np.tile([1.0, 0, 0, 0], (n, 1)), np.full(n, -2.1972246), rng.normal(size=(n, 3)))
+    t = ws.canonical_targets(base, base.copy())
+    np.testing.assert_allclose(t, ws.plain_targets(base), atol=1e-6)
+
+
+def test_scene_spec_draws_ground_truth_counts_in_range():
+    counts = [ws.scene_spec(s).gt_count for s in ws.TRAIN_SEEDS]
+    assert min(counts) >= 100_000 and max(counts) <= 250_000
+    assert len(set(counts)) > 50
+    assert not set(ws.TRAIN_SEEDS) & set(ws.EVAL_SEEDS)
+
+
+# ------------------------------------------------------------------ GPU: kernels against the oracle
+
+
+@pytest.mark.gpu
+def test_gpu_mlp_forward_matches_oracle(u3dg):
+    p = _params(11, scale=0.7).astype(np.float32)
+    x, _ = _batch(300, seed=12)
+    net = u3dg.WarmStartNet(p)
+    np.testing.assert_array_equal(net.params(), p)
+    y = net.forward(x.astype(np.float32))
+    ref, _ = wo.mlp_forward(p.astype(np.float64), x.astype(np.float32).astype(np.float64))
+    assert np.max(np.abs(y - ref)) <= 1e-5 * max(1.0, np.max(np.abs(ref))) * 10
+
+
+@pytest.mark.gpu
+def test_gpu_mlp_gradient_matches_oracle(u3dg):
+    p = _params(13, scale=0.7).astype(np.float32)
+    x, t = _batch(257, seed=14)  # not a multiple of the 64-row tile
+    x, t = x.astype(np.float32), t.astype(np.float32)
+    w = np.linspace(0.25, 1.0, wo.OUTPUTS).astype(np.float32)
+    net = u3dg.WarmStartNet(p)
+    loss, g = net.loss_grad(x, t, w)
+    rl, rg = wo.mlp_loss_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64), w.astype(np.float64))
+    assert abs(loss - rl) <= 1e-5 * rl
+    o = 0
+    for i, n in wo.LAYERS:
+        for a, b in ((o, o + i * n), (o + i * n, o + i * n + n)):
+            ok, worst = grad_close(g[a:b], rg[a:b], rel=1e-4)
+            assert ok, (i, n, a, worst)
+        o += i * n + n
+
+
+@pytest.mark.gpu
+def test_gpu_mlp_training_fits_a_teacher(u3dg):
+    rng = np.random.default_rng(15)
+    teacher = _params(16, scale=0.5)
+    x = rng.normal(size=(8192, wo.INPUTS)).astype(np.float32)
+    t, _ = wo.mlp_forward(teacher, x.astype(np.float64))
+    t = t.astype(np.float32)
+    net = u3dg.WarmStartNet(seed=3)
+    before, _ = net.loss_grad(x, t)
+    losses = net.train(x, t, epochs=30, batch=512, lr=1e-3, seed=1)
+    after, _ = net.loss_grad(x, t)
+    assert np.all(np.isfinite(losses))
+    assert after < 0.2 * before, (before, after)
+    assert losses[-1] < losses[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [1, 3, 16])
+@pytest.mark.parametrize("exclude", [False, True])
+def test_gpu_knn_matches_oracle(u3dg, k, exclude):
+    rng = np.random.default_rng(20 + k)
+    pts = rng.normal(size=(700, 3)).astype(np.float32)
+    pts[::7] = pts[1::7][:len(pts[::7])]  # duplicates: equal distances, ties by index
+    lat = (rng.integers(-2, 3, size=(100, 3)) * 0.25).astype(np.float32)
+    pts = np.concatenate([pts, lat])
+    idx, d2 = u3dg.knn(pts, pts, k, exclude_self=exclude)
+    ri, rd = wo.knn(pts, pts, k, exclude_self=exclude)
+    np.testing.assert_array_equal(idx, ri)
+    np.testing.assert_array_equal(d2, rd)
+
+
+@pytest.mark.gpu
+def test_gpu_knn_fewer_points_than_k(u3dg):
+    pts = np.array([[0, 0, 0], [1, 0, 0], [0, 2, 0]], np.float32)
+    idx, d2 = u3dg.knn(pts, pts, 16, exclude_self=True)
+    ri, rd = wo.knn(pts, pts, 16, exclude_self=True)
+    np.testing.assert_array_equal(idx, ri)
+    np.testing.assert_array_equal(d2, rd)
+    assert np.all(idx[:, 2:] == -1)
+
+
+def _tiny_scene(u3dg):
+    from univeral_3d_reconstruction_system_b200.scenes import make_scene
+    from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
+    sc = make_scene("tiny", 3)
+    imgs = u3dg.renderViewsSh(sc.truth, sc.sh_rest, 3, sc.cameras, RasterSettings())
+    sc.images = [TrainImage(c, im) for c, im in zip(sc.cameras, imgs)]
+    return sc
+
+
+@pytest.mark.gpu
+def test_gpu_features_match_oracle(u3dg):
+    sc = _tiny_scene(u3dg)
+    f = u3dg.warmstartFeatures(sc.init_xyz, sc.init_rgb, sc.images)
+    base = u3dg.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb)
+    ref = wo.features(sc.init_xyz, sc.init_rgb, np.exp(base.scales[:, 0]), sc.images)
+    # Neighbours, neighbour colours and the sampled pixels are exact; relative positions and log
+    # distances carry the plain-init sigma and a log, each within an ulp or two.
+    np.testing.assert_array_equal(f[:, 64:134], ref[:, 64:134])
+    np.testing.assert_allclose(f[:, :64], ref[:, :64], rtol=2e-6, atol=1e-6)
+    assert np.all(f[:, 133] > 0)
+
+
+@pytest.mark.gpu
+def test_gpu_warmstart_without_network_is_the_plain_init(u3dg):
+    sc = _tiny_scene(u3dg)
+    plain = u3dg.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb)
+    a = u3dg.warmstartInit(None, sc.init_xyz, sc.init_rgb, sc.images)
+    p = _params(1).astype(np.float32)
+    last = wo.PARAMS - (128 * 11 + 11)
+    p[last:last + 128 * 11] = 0.0  # zero output weights: outputs are the output biases
+    p[last + 128 * 11:] = 0.0
+    p[last + 128 * 11 + 3] = 1.0
+    p[last + 128 * 11 + 7] = np.float32(np.log(np.float32(0.1) / (np.float32(1) - np.float32(0.1))))
+    b = u3dg.warmstartInit(u3dg.WarmStartNet(p), sc.init_xyz, sc.init_rgb, sc.images)
+    for m in (a, b):
+        for name in ("means", "scales", "quats", "opacities", "colors"):
+            np.testing.assert_array_equal(getattr(m, name), getattr(plain, name), err_msg=name)
+
+
+@pytest.mark.gpu
+def test_gpu_warmstart_applies_the_network_outputs(u3dg):
+    sc = _tiny_scene(u3dg)
+    net = u3dg.WarmStartNet(_params(2, scale=0.3).astype(np.float32))
+    plain = u3dg.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb)
+    m = u3dg.warmstartInit(net, sc.init_xyz, sc.init_rgb, sc.images)
+    y = net.forward(u3dg.warmstartFeatures(sc.init_xyz, sc.init_rgb, sc.images))
+    np.testing.assert_array_equal(m.means, plain.means)
+    np.testing.assert_allclose(m.scales, plain.scales + y[:, 0:3], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(m.quats, y[:, 3:7], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(m.opacities, y[:, 7], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(m.colors, plain.colors + y[:, 8:11], rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ws.WEIGHTS_PATH.exists(), reason="trained warm-start weights not generated")
+def test_gpu_trained_network_beats_the_plain_init(u3dg):
+    """On a held-out High scene, the trained network predicts the converged fixed-set attributes better
+    than the plain initialisation does, and its initial model renders closer to the targets."""
+    sc = ws.build_scene(ws.EVAL_SEEDS[-1])
+    X, T, base = ws.label_scene(sc)
+    params, _ = ws.load_params()
+    net_loss = ws.label_loss(params, X, T)
+    w = wo.DEFAULT_WEIGHTS
+    plain_loss = float(np.sum(w * np.mean((ws.plain_targets(base).astype(np.float64) - T) ** 2, axis=0)) / 11)
+    assert net_loss < 0.8 * plain_loss, (net_loss, plain_loss)
+    warm = u3dg.warmstartInit(u3dg.WarmStartNet(params), sc.init_xyz, sc.init_rgb, sc.images)
+    psnr = []
+    for init in (base, warm):
+        t = u3dg.Trainer(init, sc.images, sc.extent, sc.options())
+        psnr.append(t.evaluatePsnr())
+        t.close()
+    assert psnr[1] > psnr[0], psnr

@@ -25,6 +25,17 @@ namespace {
 
 inline int cdiv(long long a, int b) { return int((a + b - 1) / b); }
 
+// Squared distance and dot products with every product and sum rounded on its own (no FMA
+// contraction), in a fixed order, so a host restatement reproduces neighbour order and view choice.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz)
+{
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+__device__ __forceinline__ float dot3(const float *r, float x, float y, float z)
+{
+    return __fadd_rn(__fadd_rn(__fmul_rn(r[0], x), __fmul_rn(r[1], y)), __fmul_rn(r[2], z));
+}
+
 // ------------------------------------------------------------------ k nearest neighbours
 
 // For every query, the K nearest points (squared distance, ties by lower index); candidates are
@@ -64,15 +75,17 @@ __global__ void __launch_bounds__(256) knnKernel(const float *queries, int nq, c
             const int idx = c0 + j;
             if (excludeSelf && idx == q)
                 continue;
-            const float dx = sx[j] - qx, dy = sy[j] - qy, dz = sz[j] - qz;
-            float d = dx * dx + dy * dy + dz * dz;
+            float d = dist2(sx[j] - qx, sy[j] - qy, sz[j] - qz);
             if (!(d < bd[K - 1]))
                 continue;
             int id = idx;
-            // Insertion into the sorted list (strict <: an equal distance keeps the lower index first).
+            // Insertion into the sorted list: the new entry goes before the first strictly larger one
+            // (an equal distance keeps the lower index first), and every entry after it moves down one.
+            bool shifting = false;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                if (d < bd[k]) {
+                if (shifting || d < bd[k]) {
+                    shifting = true;
                     const float td = bd[k];
                     const int ti = bi[k];
                     bd[k] = d;
@@ -110,7 +123,7 @@ __global__ void __launch_bounds__(128) featuresKernel(const float *xyz, const fl
     float *f = feat + size_t(i) * kWarmInputs;
     const float px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
     const float s = baseScale[i];
-    const float inv = s > 0.0f ? 1.0f / s : 0.0f;
+    const float inv = s > 0.0f ? __fdiv_rn(1.0f, s) : 0.0f;
     for (int k = 0; k < kWarmNeighbours; ++k) {
         const int j = nbr[size_t(i) * kWarmNeighbours + k];
         if (j < 0) {
@@ -119,9 +132,9 @@ __global__ void __launch_bounds__(128) featuresKernel(const float *xyz, const fl
             f[64 + 3 * k] = f[64 + 3 * k + 1] = f[64 + 3 * k + 2] = 0.0f;
             continue;
         }
-        f[3 * k] = (xyz[3 * j] - px) * inv;
-        f[3 * k + 1] = (xyz[3 * j + 1] - py) * inv;
-        f[3 * k + 2] = (xyz[3 * j + 2] - pz) * inv;
+        f[3 * k] = __fmul_rn(xyz[3 * j] - px, inv);
+        f[3 * k + 1] = __fmul_rn(xyz[3 * j + 1] - py, inv);
+        f[3 * k + 2] = __fmul_rn(xyz[3 * j + 2] - pz, inv);
         f[48 + k] = 0.5f * logf(fmaxf(nd2[size_t(i) * kWarmNeighbours + k], 1e-20f));
         for (int c = 0; c < 3; ++c)
             f[64 + 3 * k + c] = rgb ? rgb[3 * j + c] : 0.5f;
@@ -138,20 +151,26 @@ __global__ void __launch_bounds__(128) featuresKernel(const float *xyz, const fl
     for (int v = 0; v < nViews; ++v) {
         const ViewRef &vr = views[v];
         const float *R = vr.cam.R;
-        const float x = R[0] * px + R[1] * py + R[2] * pz + vr.cam.t[0];
-        const float y = R[3] * px + R[4] * py + R[5] * pz + vr.cam.t[1];
-        const float z = R[6] * px + R[7] * py + R[8] * pz + vr.cam.t[2];
+        const float x = __fadd_rn(dot3(R, px, py, pz), vr.cam.t[0]);
+        const float y = __fadd_rn(dot3(R + 3, px, py, pz), vr.cam.t[1]);
+        const float z = __fadd_rn(dot3(R + 6, px, py, pz), vr.cam.t[2]);
         if (!(z > 1e-3f))
             continue;
-        const int u = __float2int_rn(vr.cam.fx * x / z + vr.cam.cx);
-        const int w = __float2int_rn(vr.cam.fy * y / z + vr.cam.cy);
+        const float uf = __fadd_rn(__fdiv_rn(__fmul_rn(vr.cam.fx, x), z), vr.cam.cx);
+        const float wf = __fadd_rn(__fdiv_rn(__fmul_rn(vr.cam.fy, y), z), vr.cam.cy);
+        // Inside the image (also rejects non-finite coordinates before the integer conversion).
+        if (!(uf > -0.5f && wf > -0.5f && uf < float(vr.cam.width) - 0.5f && wf < float(vr.cam.height) - 0.5f))
+            continue;
+        const int u = __float2int_rn(uf);
+        const int w = __float2int_rn(wf);
         if (u < 0 || w < 0 || u >= vr.cam.width || w >= vr.cam.height)
             continue;
-        const float dx = px - vr.cx, dy = py - vr.cy, dz = pz - vr.cz;
-        float d = dx * dx + dy * dy + dz * dz;
+        float d = dist2(px - vr.cx, py - vr.cy, pz - vr.cz);
         int vv = v, uu = u, ww = w;
+        bool shifting = false; // insertion as in knnKernel: ties keep the lower view index first
         for (int k = 0; k < kWarmViews; ++k) {
-            if (d < bd[k]) {
+            if (shifting || d < bd[k]) {
+                shifting = true;
                 const float td = bd[k];
                 const int tv = bv[k], tu = bu[k], tw = bw[k];
                 bd[k] = d;
@@ -172,7 +191,7 @@ __global__ void __launch_bounds__(128) featuresKernel(const float *xyz, const fl
             const ViewRef &vr = views[bv[k]];
             const uint8_t *px8 = vr.rgb + (size_t(bw[k]) * vr.cam.width + bu[k]) * 3;
             for (int c = 0; c < 3; ++c)
-                c3[c] = float(px8[c]) * (1.0f / 255.0f) - 0.5f;
+                c3[c] = __fadd_rn(__fmul_rn(float(px8[c]), 1.0f / 255.0f), -0.5f);
             ++seen;
         }
         for (int c = 0; c < 3; ++c)
