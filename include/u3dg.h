@@ -259,6 +259,16 @@ int u3dg_photometric_loss(const float *render, const float *target, int width, i
                           float *grad, u3dg_loss_value *out);
 /* psnr (Loss.h:21, Loss.cpp:187-196): double accumulation, 99 dB when MSE <= 1e-12. */
 int u3dg_psnr(const float *a, const float *b, size_t count, float *out);
+/* No reference counterpart: u3dg_photometric_loss on DEVICE pointers (render, target, grad are
+ * height*width*3 floats in device memory of the current device) that allocates nothing. Temporaries
+ * live in a fixed 11.1 MB device array per device, so width*height must be <= 640*480 and the image
+ * at most 2048 loss blocks of 32x16 pixels; larger images return U3DG_ERR_CAPACITY. Work runs on
+ * `stream` (a cudaStream_t; NULL = the default stream), and the call synchronises it before
+ * returning. The first call on a device resolves the array's address there; make it before any
+ * stream capture begins on that device. Calls on one device share the array and are serialised by
+ * a per-device lock. Same results as u3dg_photometric_loss. */
+int u3dg_photometric_loss_noalloc(const float *render, const float *target, int width, int height, float lambda,
+                                  float *grad, u3dg_loss_value *out, void *stream);
 
 /* ------------------------------------------------------------------ Adam */
 

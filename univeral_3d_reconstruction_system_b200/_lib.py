@@ -72,6 +72,8 @@ SIGNATURES = {
                                          _SZ, _I]),
     "u3dg_photometric_loss": (C.c_int, [_F, _F, C.c_int, C.c_int, C.c_float, _F, C.POINTER(_abi.LossValue)]),
     "u3dg_psnr": (C.c_int, [_F, _F, C.c_size_t, _F]),
+    "u3dg_photometric_loss_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, _P, C.POINTER(_abi.LossValue),
+                                                _P]),
     "u3dg_adam_create": (C.c_int, [C.c_size_t, _PP]),
     "u3dg_adam_step": (C.c_int, [_P, _MV, _MV, C.POINTER(_abi.LearningRates)]),
     "u3dg_adam_compact": (C.c_int, [_P, _abi.u8p, C.c_size_t]),
