@@ -19,6 +19,7 @@ the single-scene path has no collective).
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -297,7 +298,59 @@ def run_ours(args, dist: Dist) -> dict:
         res["schedule"] = run_full_schedule(args, sc)
     if args.warmstart and dist.world == 1:
         res["warmstart"] = run_warmstart(args)
+    if args.batched:
+        res["batched"] = run_batched(args)
     return res
+
+
+def run_batched(args) -> dict:
+    """Batched multi-scene training: 16 seeded scenes (scenes.batched_specs) trained together by one
+    u3dg_batch (per-scene streams, step graphs, tile sizes from the autotuner), then each scene alone
+    with its tuned tile size. Reports the aggregate iterations/s of both and every scene's PSNR."""
+    from univeral_3d_reconstruction_system_b200 import api
+    from univeral_3d_reconstruction_system_b200.scenes import batched_specs, make_scene
+    from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
+
+    t0 = time.time()
+    scenes, specs = [], batched_specs(0, 16)
+    for k, sp in enumerate(specs):
+        sc = make_scene(sp, 500 + k)
+        imgs = api.renderViewsSh(sc.truth, sc.sh_rest, 3, sc.cameras, RasterSettings())
+        sc.images = [TrainImage(c, im) for c, im in zip(sc.cameras, imgs)]
+        opt = sc.options()
+        if args.batched_iterations > 0:
+            opt.iterations = min(opt.iterations, args.batched_iterations)
+        scenes.append((api.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb), sc.images, sc.extent, opt))
+    log(f"batched: 16 scenes built in {time.time() - t0:.1f} s")
+    t1 = time.time()
+    b = api.Batch(scenes, autotune=True)
+    tune_s = time.time() - t1
+    total = sum(opt.iterations for _, _, _, opt in scenes)
+    ms = b.time_steps(max(opt.iterations for _, _, _, opt in scenes))
+    rows = []
+    seq_ms = 0.0
+    for k, (init, imgs, extent, opt) in enumerate(scenes):
+        tile, tuned = b.tile_size(k)
+        tb = b.trainer(k)
+        p_batch = tb.evaluatePsnr()
+        o2 = dataclasses.replace(opt, raster=dataclasses.replace(opt.raster, tile_size=tile))
+        t = api.Trainer(init, imgs, extent, o2)
+        seq_ms += t.time_steps(opt.iterations)
+        p_alone = t.evaluatePsnr()
+        rows.append({"scene": specs[k].name, "gt": specs[k].gt_count, "views": specs[k].views,
+                     "width": specs[k].width, "iterations": opt.iterations, "tile": tile,
+                     "tuned_ms_per_step": round(tuned, 4), "gaussians": tb.size(), "psnr_batched": round(p_batch, 4),
+                     "psnr_alone": round(p_alone, 4)})
+        t.close()
+    b.close()
+    diffs = [abs(r["psnr_batched"] - r["psnr_alone"]) for r in rows]
+    out = {"scenes": 16, "iterations_total": total, "batched_ms": round(ms, 2),
+           "batched_it_per_s": round(total / (ms * 1e-3), 1), "sequential_ms": round(seq_ms, 2),
+           "sequential_it_per_s": round(total / (seq_ms * 1e-3), 1), "speedup": round(seq_ms / ms, 3),
+           "autotune_s": round(tune_s, 2), "max_psnr_diff_db": round(max(diffs), 5), "per_scene": rows}
+    log(f"batched: {out['batched_it_per_s']} it/s vs sequential {out['sequential_it_per_s']} it/s, "
+        f"max PSNR diff {out['max_psnr_diff_db']} dB")
+    return out
 
 
 def run_warmstart(args) -> dict | None:
@@ -421,6 +474,10 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="high-300k")
     ap.add_argument("--no-schedule", dest="schedule", action="store_false",
                     help="skip the full-schedule run (PSNR trajectory, time to PSNR)")
+    ap.add_argument("--batched", action="store_true",
+                    help="also run the 16-scene batched workload against the same scenes trained alone")
+    ap.add_argument("--batched-iterations", type=int, default=0,
+                    help="cap on each batched scene's schedule (0: the preset schedules)")
     ap.add_argument("--no-warmstart", dest="warmstart", action="store_false",
                     help="skip the learned warm-start vs plain comparison")
     ap.add_argument("--ncu-steps", type=int, default=0,
@@ -443,7 +500,7 @@ def main():
                 "config": config(args, dist), "roofline": res["roofline"], "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "phase_ms": res["phase_ms"],
                 "workload_stats": res["workload_stats"]}
-        for key in ("schedule", "warmstart"):
+        for key in ("schedule", "warmstart", "batched"):
             if key in res:
                 line[key] = res[key]
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

@@ -202,6 +202,13 @@ int u3dg_trainer_replays(u3dg_trainer *trainer, int *replays);
 /* Device time in milliseconds of `count` steps, measured with CUDA events recorded on the
  * trainer's stream right before the first and after the last step (host waits on both sides). */
 int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms);
+/* No reference counterpart. Runs of 10 steps with no densification, opacity reset or profiling
+ * among them, when every view has the same size, are launched as one CUDA graph whose kernels read
+ * each step's view and learning rates from device memory (on by default; results are identical to
+ * step-by-step launches). set_graphs turns this on (1) or off (0); graph_launches reports how many
+ * graph launches ran so far. */
+int u3dg_trainer_set_graphs(u3dg_trainer *trainer, int enable);
+int u3dg_trainer_graph_launches(u3dg_trainer *trainer, long long *launches);
 void u3dg_trainer_destroy(u3dg_trainer *trainer);
 
 /* ------------------------------------------------------------------ rasterizer (unit boundary) */
@@ -249,6 +256,29 @@ int u3dg_densify_and_prune(u3dg_model *model, u3dg_model *adam_m, u3dg_model *ad
                            const int *grad_count, size_t capacity, float scene_extent,
                            const u3dg_train_options *options, int opacity_was_reset, unsigned int seed, size_t *count,
                            int *counts3);
+
+/* ------------------------------------------------------------------ batched training */
+
+/* No reference counterpart (the reference trains one scene per Trainer). Trains `scenes` scenes at
+ * once on the current device: scene s starts from initial[s] with images[s][0 .. image_counts[s])
+ * and options[s] (each with its own schedule and Gaussian cap). Every scene keeps its own trainer and
+ * stream; u3dg_batch_step advances each scene by `count` iterations (or to its end), interleaving the
+ * scenes so their kernels run concurrently and running steps through each scene's step graph where
+ * it can. With autotune != 0, each scene's tile size (8, 16 or 32) is chosen at creation from short
+ * timed runs on throwaway trainers; tile_size reports it and the tuned ms per step. batch_trainer
+ * returns a borrowed handle for the per-scene queries of the u3dg_trainer_* API (download, stats,
+ * eval_psnr, ...); destroying it is a no-op, the batch owns it. time_steps steps like batch_step and
+ * reports the device time from one event that all scene streams wait on to the last stream's end. */
+typedef struct u3dg_batch u3dg_batch;
+int u3dg_batch_create(const u3dg_model *initial, const u3dg_image *const *images, const int *image_counts,
+                      const float *extents, const u3dg_train_options *options, int scenes, int autotune,
+                      u3dg_batch **out);
+int u3dg_batch_step(u3dg_batch *batch, int count);
+int u3dg_batch_time_steps(u3dg_batch *batch, int count, float *ms);
+int u3dg_batch_size(u3dg_batch *batch, int *scenes);
+int u3dg_batch_trainer(u3dg_batch *batch, int scene, u3dg_trainer **out);
+int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_ms_per_step);
+void u3dg_batch_destroy(u3dg_batch *batch);
 
 /* ------------------------------------------------------------------ loss */
 

@@ -386,6 +386,30 @@ def test_overflow_replay_is_exact(u3dg, oracle, tiny_scene):
     np.testing.assert_array_equal(a.model().flat(), b.model().flat())
 
 
+def test_graph_steps_match_step_by_step_launches(u3dg, oracle, tiny_scene):
+    """Runs of 10 steps launched as one CUDA graph (kernels reading each step's view and learning rates
+    from device descriptors) give bit-identical models to step-by-step launches, through a
+    densification and with overflow replays inside graph runs."""
+    sc = tiny_scene
+    init = oracle.init_from_points(sc.init_xyz, sc.init_rgb)
+    opt = sc.options()
+    runs = []
+    for graphs, capacity in ((False, 0), (True, 0), (True, 1024)):
+        t = u3dg.Trainer(init, sc.images, sc.extent, opt)
+        t.set_graphs(graphs)
+        if capacity:
+            t.set_intersection_capacity(capacity)
+        t.step(57)
+        t.step(100)
+        runs.append((t.model().flat(), t.stats(), t.graph_launches(), t.replays()))
+    assert runs[0][2] == 0 and runs[1][2] >= 10 and runs[2][2] >= 5
+    assert runs[2][3] >= 1
+    for flat, st, _, _ in runs[1:]:
+        np.testing.assert_array_equal(flat, runs[0][0])
+        assert (st.iteration, st.loss, st.psnr, st.gaussians) == (runs[0][1].iteration, runs[0][1].loss,
+                                                                   runs[0][1].psnr, runs[0][1].gaussians)
+
+
 def test_training_recovers_a_synthetic_scene(u3dg, oracle):
     """training_recovers_a_synthetic_scene (test_splat.cpp:227-268) on the GPU."""
     rng = np.random.default_rng(11)

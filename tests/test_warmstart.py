@@ -35,6 +35,7 @@ def _batch(n, seed=1):
 
 def test_param_count_matches_header():
     assert wo.PARAMS == 51723
+    np.testing.assert_array_equal(ws.LOSS_WEIGHTS, wo.DEFAULT_WEIGHTS)
 
 
 def test_oracle_mlp_gradient_matches_central_differences():
@@ -259,18 +260,20 @@ def test_gpu_warmstart_applies_the_network_outputs(u3dg):
 @pytest.mark.skipif(not ws.WEIGHTS_PATH.exists(), reason="trained warm-start weights not generated")
 def test_gpu_trained_network_beats_the_plain_init(u3dg):
     """On a held-out High scene, the trained network predicts the converged fixed-set attributes better
-    than the plain initialisation does, and its initial model renders closer to the targets."""
+    than the plain initialisation does, and training from its initial model is ahead of training from
+    the plain one after 1000 iterations of the same schedule (by about 0.6 dB on the held-out seeds)."""
     sc = ws.build_scene(ws.EVAL_SEEDS[-1])
     X, T, base = ws.label_scene(sc)
     params, _ = ws.load_params()
     net_loss = ws.label_loss(params, X, T)
-    w = wo.DEFAULT_WEIGHTS
+    w = ws.LOSS_WEIGHTS
     plain_loss = float(np.sum(w * np.mean((ws.plain_targets(base).astype(np.float64) - T) ** 2, axis=0)) / 11)
     assert net_loss < 0.8 * plain_loss, (net_loss, plain_loss)
     warm = u3dg.warmstartInit(u3dg.WarmStartNet(params), sc.init_xyz, sc.init_rgb, sc.images)
     psnr = []
     for init in (base, warm):
         t = u3dg.Trainer(init, sc.images, sc.extent, sc.options())
+        t.step(1000)
         psnr.append(t.evaluatePsnr())
         t.close()
-    assert psnr[1] > psnr[0], psnr
+    assert psnr[1] > psnr[0] + 0.1, psnr

@@ -58,6 +58,8 @@ SIGNATURES = {
     "u3dg_trainer_time_steps": (C.c_int, [_P, C.c_int, _F]),
     "u3dg_trainer_set_intersection_capacity": (C.c_int, [_P, C.c_size_t]),
     "u3dg_trainer_replays": (C.c_int, [_P, _I]),
+    "u3dg_trainer_set_graphs": (C.c_int, [_P, C.c_int]),
+    "u3dg_trainer_graph_launches": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "u3dg_trainer_destroy": (None, [_P]),
     "u3dg_rasterizer_create": (C.c_int, [_PP]),
     "u3dg_rasterizer_forward": (C.c_int, [_P, _MV, _CAM, _ST, _F]),
@@ -70,6 +72,13 @@ SIGNATURES = {
     "u3dg_bin_tiles": (C.c_int, [_F, _I, _I, C.c_size_t, C.c_int, C.c_int, _I, _I, C.c_size_t, _SZ]),
     "u3dg_densify_and_prune": (C.c_int, [_MV, _MV, _MV, _F, _I, C.c_size_t, C.c_float, _OPT, C.c_int, C.c_uint,
                                          _SZ, _I]),
+    "u3dg_batch_create": (C.c_int, [_MV, C.POINTER(C.POINTER(_abi.Image)), _I, _F, _OPT, C.c_int, C.c_int, _PP]),
+    "u3dg_batch_step": (C.c_int, [_P, C.c_int]),
+    "u3dg_batch_time_steps": (C.c_int, [_P, C.c_int, _F]),
+    "u3dg_batch_size": (C.c_int, [_P, _I]),
+    "u3dg_batch_trainer": (C.c_int, [_P, C.c_int, _PP]),
+    "u3dg_batch_tile_size": (C.c_int, [_P, C.c_int, _I, _F]),
+    "u3dg_batch_destroy": (None, [_P]),
     "u3dg_photometric_loss": (C.c_int, [_F, _F, C.c_int, C.c_int, C.c_float, _F, C.POINTER(_abi.LossValue)]),
     "u3dg_psnr": (C.c_int, [_F, _F, C.c_size_t, _F]),
     "u3dg_photometric_loss_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, _P, C.POINTER(_abi.LossValue),

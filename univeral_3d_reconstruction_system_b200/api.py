@@ -127,6 +127,15 @@ class Trainer:
         check(load().u3dg_trainer_replays(self._h, C.byref(r)))
         return r.value
 
+    def set_graphs(self, enable: bool) -> None:
+        """Graph launches of 10-step runs without densification (identical results either way)."""
+        check(load().u3dg_trainer_set_graphs(self._h, 1 if enable else 0))
+
+    def graph_launches(self) -> int:
+        v = C.c_longlong()
+        check(load().u3dg_trainer_graph_launches(self._h, C.byref(v)))
+        return int(v.value)
+
     def set_profiling(self, enable: bool) -> None:
         check(load().u3dg_trainer_set_profiling(self._h, 1 if enable else 0))
 
@@ -134,6 +143,80 @@ class Trainer:
         t = _abi.PhaseTimes()
         check(load().u3dg_trainer_phase_times(self._h, C.byref(t)))
         return {name: getattr(t, name) for name, _ in t._fields_}
+
+
+class Batch:
+    """Many scenes trained at once on one GPU (u3dg_batch_*; no reference counterpart).
+
+    scenes: a list of (initial GaussianModel, images, scene extent, TrainOptions). Each scene keeps its
+    own trainer and stream; step() advances every scene by `count` iterations, interleaving them so
+    their kernels run concurrently. With autotune, each scene's tile size (8, 16 or 32) is picked at
+    creation from short timed runs."""
+
+    def __init__(self, scenes, autotune: bool = True):
+        L = load()
+        S = len(scenes)
+        if S == 0:
+            raise ValueError("no scenes")
+        models = (_abi.ModelView * S)()
+        images = (C.POINTER(_abi.Image) * S)()
+        counts = (C.c_int32 * S)()
+        extents = (C.c_float * S)()
+        opts = (_abi.TrainOptions * S)()
+        keep = []
+        self._scenes = []
+        for k, (init, imgs, extent, options) in enumerate(scenes):
+            imgs = list(imgs)
+            models[k] = init.view()
+            arr, kp = images_struct(imgs)
+            keep += [init, arr, kp]
+            images[k] = C.cast(arr, C.POINTER(_abi.Image))
+            counts[k] = len(imgs)
+            extents[k] = float(extent)
+            options = options or TrainOptions()
+            opts[k] = options.struct()
+            self._scenes.append((imgs, options))
+        h = C.c_void_p()
+        check(L.u3dg_batch_create(models, images, counts, extents, opts, S, 1 if autotune else 0, C.byref(h)))
+        self._h = h
+        del keep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            load().u3dg_batch_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def __len__(self) -> int:
+        return len(self._scenes)
+
+    def step(self, count: int = 1) -> None:
+        check(load().u3dg_batch_step(self._h, count))
+
+    def time_steps(self, count: int) -> float:
+        """Device milliseconds of `count` iterations of every scene."""
+        ms = C.c_float()
+        check(load().u3dg_batch_time_steps(self._h, count, C.byref(ms)))
+        return float(ms.value)
+
+    def tile_size(self, scene: int):
+        """(tile size, tuned ms per step) of a scene."""
+        tile, ms = C.c_int32(), C.c_float()
+        check(load().u3dg_batch_tile_size(self._h, scene, C.byref(tile), C.byref(ms)))
+        return int(tile.value), float(ms.value)
+
+    def trainer(self, scene: int) -> "Trainer":
+        """The scene's trainer (borrowed: valid while this batch is alive)."""
+        h = C.c_void_p()
+        check(load().u3dg_batch_trainer(self._h, scene, C.byref(h)))
+        t = Trainer.__new__(Trainer)
+        t._h = h
+        t._images, t._options = self._scenes[scene]
+        t._owner = self
+        return t
 
 
 class Rasterizer:

@@ -252,8 +252,10 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
 // Capacity check of this bin pass: the usable count is the scan total, or 0 when it exceeds the
 // intersection buffers or a previous step already aborted (the abort is sticky until the host
 // clears it). iteration identifies the aborted step for the host.
-__global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int iteration)
+__global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int iteration, const StepDesc *desc)
 {
+    if (desc)
+        iteration = desc->iteration;
     const int t = *total;
     const bool over = t < 0 || t > capacity;
     if (over) {
@@ -372,9 +374,10 @@ void launchSetCount(BinCounts *c, int n, cudaStream_t s)
     { setCountKernel<<<1, 1, 0, s>>>(c, n); countLaunch(); }
 }
 
-void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s)
+void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
+                         const StepDesc *desc)
 {
-    { capacityKernel<<<1, 1, 0, s>>>(total, capacity, c, iteration); countLaunch(); }
+    { capacityKernel<<<1, 1, 0, s>>>(total, capacity, c, iteration, desc); countLaunch(); }
 }
 
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,

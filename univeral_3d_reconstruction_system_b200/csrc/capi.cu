@@ -85,10 +85,6 @@ struct Stream {
 
 } // namespace
 
-struct u3dg_trainer {
-    std::unique_ptr<TrainerImpl> impl;
-};
-
 struct u3dg_rasterizer {
     int device = 0;
     Stream stream;
@@ -361,6 +357,26 @@ int u3dg_trainer_replays(u3dg_trainer *trainer, int *replays)
     });
 }
 
+int u3dg_trainer_set_graphs(u3dg_trainer *trainer, int enable)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        t.useGraphs = enable != 0;
+        if (!t.useGraphs)
+            t.stepGraph.reset();
+    });
+}
+
+int u3dg_trainer_graph_launches(u3dg_trainer *trainer, long long *launches)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        if (!launches)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "launches is NULL");
+        *launches = t.graphChunks;
+    });
+}
+
 int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms)
 {
     return guarded([&] {
@@ -384,7 +400,7 @@ int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms)
 
 void u3dg_trainer_destroy(u3dg_trainer *trainer)
 {
-    if (!trainer)
+    if (!trainer || trainer->ownedByBatch)
         return;
     try {
         if (trainer->impl)

@@ -26,6 +26,14 @@ void countLaunch() { gLaunches.fetch_add(1, std::memory_order_relaxed); }
 
 unsigned long long launchCount() { return gLaunches.load(std::memory_order_relaxed); }
 
+void addLaunches(long long k) { gLaunches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
+
+static std::atomic<unsigned long long> gAllocEpoch{0};
+
+unsigned long long allocEpoch() { return gAllocEpoch.load(std::memory_order_relaxed); }
+
+void bumpAllocEpoch() { gAllocEpoch.fetch_add(1, std::memory_order_relaxed); }
+
 static thread_local std::string tLastError;
 
 int setError(int code, const std::string &msg)
@@ -94,7 +102,7 @@ void RasterWorkspace::reserveIntersections(size_t capacity)
 }
 
 void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
-                              const float *shRest, int shDegree, cudaStream_t stream)
+                              const float *shRest, int shDegree, cudaStream_t stream, const StepDesc *desc)
 {
     checkSettings(s);
     checkCamera(c);
@@ -121,10 +129,10 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     if (icap == 0)
         reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * nn));
     ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
-    launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream);
+    launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
 }
 
-void RasterWorkspace::bin(cudaStream_t stream, int iteration)
+void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *desc)
 {
     const int tiles = tilesX * tilesY;
     hist.reserve(std::max(radixHistEntries(std::max(n, icap)), size_t(256)));
@@ -137,7 +145,7 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration)
     sortedIds = valsOut;
     launchRankCounts(sortedIds, rect.p, radius.p, n, cnt.p, rankOf.p, stream);
     exclusiveScan(cnt.p, offs.p, n, scanPartial.p, stream);
-    launchCapacityCheck(offs.p + n, icap, counts.p, iteration, stream);
+    launchCapacityCheck(offs.p + n, icap, counts.p, iteration, stream, desc);
     launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, iKeys0.p, emitGid.p, stream);
     int bits = 0;
     while ((1 << bits) < tiles)
@@ -293,6 +301,12 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     std::memset(hStats.p, 0, sizeof(DevStats));
     hCounts.reserve(4);
     statusSlots.reserve(kSlots);
+    uniformViews = !cams.empty();
+    for (const u3dg_camera &c : cams)
+        uniformViews = uniformViews && c.width == cams[0].width && c.height == cams[0].height;
+    descDev.reserve(kGraphSteps, true);
+    descHost.reserve(kGraphSteps);
+    graphStatus.reserve(kGraphSteps);
     // Intersection buffers sized for 16 tiles per Gaussian at the capacity; they grow on demand.
     ws.reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * cap));
     // The host buffers of the caller may be released after this call returns.
@@ -376,8 +390,15 @@ void TrainerImpl::step()
 void TrainerImpl::stepTo(int target)
 {
     target = std::min(target, o.iterations);
-    while (iteration < target && !cams.empty())
+    while (iteration < target && !cams.empty()) {
+        if (graphEligible(target)) {
+            finish(); // graph chunks start with no step in flight
+            if (graphEligible(target))
+                runGraphChunk(); // false: rolled back or not captured; the loop goes on from the restored state
+            continue;
+        }
         step();
+    }
 }
 
 void TrainerImpl::finish()
@@ -396,10 +417,9 @@ void TrainerImpl::finish()
     }
 }
 
-void TrainerImpl::enqueueStep()
+StepValues TrainerImpl::nextStep()
 {
-    InFlight f;
-    f.snap = snapshot();
+    StepValues sv;
     // View order: one shuffle of all views per epoch (Trainer.cpp:57-64).
     if (orderPos >= order.size()) {
         order.resize(cams.size());
@@ -408,17 +428,35 @@ void TrainerImpl::enqueueStep()
         std::shuffle(order.begin(), order.end(), rng);
         orderPos = 0;
     }
-    const size_t v = size_t(order[orderPos++]);
-    const u3dg_camera &cam = cams[v];
-    const uint8_t *target = images.p + imageOffset[v];
+    sv.view = size_t(order[orderPos++]);
+    sv.d.cam = cams[sv.view];
+    sv.d.target = images.p + imageOffset[sv.view];
+    sv.d.iteration = iteration;
+    // Means learning rate decays exponentially and scales with the scene (Trainer.cpp:81-85);
+    // Adam bias corrections as Adam::step (Adam.cpp:68-71), all in host float like the reference.
+    const float t = float(iteration) / float(std::max(1, o.iterations - 1));
+    const float lrMeans = std::exp(std::log(o.lr.means) * (1 - t) + std::log(o.means_lr_final) * t) * extent;
+    ++adamStep;
+    const float bc1 = 1.0f - std::pow(0.9f, float(adamStep));
+    const float bc2 = 1.0f - std::pow(0.999f, float(adamStep));
+    const float lrs[5] = {lrMeans, o.lr.scales, o.lr.quats, o.lr.opacities, o.lr.colors};
+    for (int k = 0; k < 5; ++k)
+        sv.d.stepSize[k] = lrs[k] / bc1;
+    sv.d.invSqrtBc2 = 1.0f / std::sqrt(bc2);
+    return sv;
+}
+
+void TrainerImpl::launchStep(const StepValues &sv, const StepDesc *desc, BinCounts *statusDst)
+{
+    const u3dg_camera &cam = sv.d.cam;
     const int W = cam.width, H = cam.height;
-    PhaseTimer *tm = profiling ? timer : nullptr;
+    PhaseTimer *tm = (profiling && !desc) ? timer : nullptr;
     if (tm)
         tm->mark(0, stream);
-    ws.project(params(), n, cam, o.raster, nullptr, 0, stream);
+    ws.project(params(), n, cam, o.raster, nullptr, 0, stream, desc);
     if (tm)
         tm->mark(1, stream);
-    ws.bin(stream, iteration);
+    ws.bin(stream, sv.d.iteration, desc);
     if (tm)
         tm->mark(2, stream);
     ws.composite(stream);
@@ -428,37 +466,40 @@ void TrainerImpl::enqueueStep()
     const int lb = lossBlocks(W, H);
     lossBlockSums.reserve(size_t(lb) * 3);
     LossScratch ls{abc.p, lossBlockSums.p, lb};
-    launchLoss(ws.rgb.p, nullptr, target, W, H, o.ssim_lambda, dLoss.p, ls, stream);
-    launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, iteration + 1, ws.counts.p, nullptr, nullptr, stream);
+    launchLoss(ws.rgb.p, nullptr, sv.d.target, W, H, o.ssim_lambda, dLoss.p, ls, stream, desc);
+    launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, sv.d.iteration + 1, ws.counts.p, nullptr, nullptr, stream,
+                       desc);
     if (tm)
         tm->mark(4, stream);
     ws.backwardComposite(dLoss.p, stream);
     if (tm)
         tm->mark(5, stream);
-    // Means learning rate decays exponentially and scales with the scene (Trainer.cpp:81-85);
-    // Adam bias corrections as Adam::step (Adam.cpp:68-71), all in host float like the reference.
-    const float t = float(iteration) / float(std::max(1, o.iterations - 1));
-    const float lrMeans = std::exp(std::log(o.lr.means) * (1 - t) + std::log(o.means_lr_final) * t) * extent;
-    ++adamStep;
-    const float bc1 = 1.0f - std::pow(0.9f, float(adamStep));
-    const float bc2 = 1.0f - std::pow(0.999f, float(adamStep));
     ChainArgs a = ws.chainArgs(params());
     a.gradAccum = gradAccum.p;
     a.gradCount = gradCount.p;
     a.m = moment1();
     a.v = moment2();
-    const float lrs[5] = {lrMeans, o.lr.scales, o.lr.quats, o.lr.opacities, o.lr.colors};
     for (int k = 0; k < 5; ++k)
-        a.stepSize[k] = lrs[k] / bc1;
-    a.invSqrtBc2 = 1.0f / std::sqrt(bc2);
+        a.stepSize[k] = sv.d.stepSize[k];
+    a.invSqrtBc2 = sv.d.invSqrtBc2;
+    a.desc = desc;
     launchChain(a, true, stream);
     U3DG_CUDA(cudaGetLastError());
     if (tm)
         tm->mark(6, stream);
-    ++iteration;
+    U3DG_CUDA(cudaMemcpyAsync(statusDst, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, stream));
+}
+
+void TrainerImpl::enqueueStep()
+{
+    InFlight f;
+    f.snap = snapshot();
+    const StepValues sv = nextStep();
     f.slot = nextSlot;
     nextSlot = (nextSlot + 1) % kSlots;
-    U3DG_CUDA(cudaMemcpyAsync(statusSlots.p + f.slot, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, stream));
+    launchStep(sv, nullptr, statusSlots.p + f.slot);
+    ++normalSteps;
+    ++iteration;
     if (freeEvents.empty()) {
         cudaEvent_t e;
         U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -480,6 +521,7 @@ void TrainerImpl::enqueueStep()
     if (o.opacity_reset_interval > 0 && iteration < o.refine_stop && iteration % o.opacity_reset_interval == 0)
         resetOpacity();
     U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
+    PhaseTimer *tm = profiling ? timer : nullptr;
     if (tm) {
         tm->mark(7, stream);
         U3DG_CUDA(cudaEventSynchronize(tm->ev[7]));
@@ -496,8 +538,181 @@ void TrainerImpl::enqueueStep()
         U3DG_CUDA(cudaMemcpy(ws.hostCounts.p, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost));
         acc.intersections += uint64_t(std::max(ws.hostCounts.p->effTotal, 0));
         acc.gaussians += uint64_t(ws.n);
-        acc.pixels += uint64_t(W) * uint64_t(H);
+        acc.pixels += uint64_t(sv.d.cam.width) * uint64_t(sv.d.cam.height);
     }
+}
+
+bool TrainerImpl::graphEligible(int target) const
+{
+    if (!useGraphs || profiling || !uniformViews || normalSteps == 0 || iteration + kGraphSteps > target)
+        return false;
+    for (int j = 1; j <= kGraphSteps; ++j) {
+        const int it = iteration + j;
+        if (it >= o.refine_start && it < o.refine_stop && it % o.refine_interval == 0)
+            return false;
+        if (o.opacity_reset_interval > 0 && it < o.refine_stop && it % o.opacity_reset_interval == 0)
+            return false;
+    }
+    return true;
+}
+
+bool TrainerImpl::runGraphChunk()
+{
+    if (!beginGraphChunk())
+        return false;
+    return endGraphChunk();
+}
+
+bool TrainerImpl::beginGraphChunk()
+{
+    constexpr int K = kGraphSteps;
+    pendingSnaps.assign(K, HostSnapshot{});
+    StepValues vals[K];
+    for (int k = 0; k < K; ++k) {
+        pendingSnaps[k] = snapshot();
+        vals[k] = nextStep();
+        descHost.p[k] = vals[k].d;
+        ++iteration;
+    }
+    const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
+                       stepGraph.icap != ws.icap || stepGraph.epoch != allocEpoch();
+    if (stale) {
+        stepGraph.reset();
+        const unsigned long long epoch0 = allocEpoch();
+        const unsigned long long launches0 = launchCount();
+        U3DG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+        try {
+            for (int k = 0; k < K; ++k)
+                launchStep(vals[k], descDev.p + k, graphStatus.p + k);
+            U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream, &g);
+            if (g)
+                cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        U3DG_CUDA(cudaStreamEndCapture(stream, &stepGraph.graph));
+        // The captured kernels ran no work yet: count them when the graph runs.
+        stepGraph.kernels = (long long)(launchCount() - launches0);
+        addLaunches(-stepGraph.kernels);
+        if (allocEpoch() != epoch0) {
+            // A buffer moved while the steps were being recorded: the graph may hold stale addresses.
+            stepGraph.reset();
+            restore(pendingSnaps[0]);
+            pendingSnaps.clear();
+            return false;
+        }
+        U3DG_CUDA(cudaGraphInstantiate(&stepGraph.exec, stepGraph.graph, 0));
+        stepGraph.n = n;
+        stepGraph.cur = cur;
+        stepGraph.icap = ws.icap;
+        stepGraph.epoch = allocEpoch();
+    }
+    U3DG_CUDA(cudaMemcpyAsync(descDev.p, descHost.p, K * sizeof(StepDesc), cudaMemcpyHostToDevice, stream));
+    U3DG_CUDA(cudaGraphLaunch(stepGraph.exec, stream));
+    addLaunches(stepGraph.kernels);
+    ++graphChunks;
+    return true;
+}
+
+bool TrainerImpl::endGraphChunk()
+{
+    sync();
+    const int K = int(pendingSnaps.size());
+    for (int k = 0; k < K; ++k) {
+        const BinCounts c = graphStatus.p[k];
+        if (c.abortIter >= 0) {
+            // Step k overflowed: it and the steps after it did nothing on the device.
+            restore(pendingSnaps[k]);
+            pendingSnaps.clear();
+            ws.reserveIntersections(size_t(c.need) + size_t(c.need) / 2);
+            ws.clearCounts(stream);
+            ++replays;
+            return false;
+        }
+        if (size_t(c.total) + size_t(c.total) / 4 > size_t(ws.icap))
+            ws.reserveIntersections(size_t(c.total) + size_t(c.total) / 2);
+    }
+    pendingSnaps.clear();
+    return true;
+}
+
+void stepBatch(const std::vector<TrainerImpl *> &trainers, int count)
+{
+    const size_t S = trainers.size();
+    std::vector<int> target(S);
+    for (size_t i = 0; i < S; ++i)
+        target[i] = std::min(trainers[i]->iteration + std::max(count, 0), trainers[i]->o.iterations);
+    std::vector<char> launched(S);
+    for (;;) {
+        bool any = false;
+        std::fill(launched.begin(), launched.end(), 0);
+        for (size_t i = 0; i < S; ++i) {
+            TrainerImpl &t = *trainers[i];
+            if (t.iteration >= target[i] || t.cams.empty())
+                continue;
+            any = true;
+            U3DG_CUDA(cudaSetDevice(t.device));
+            if (t.graphEligible(target[i])) {
+                t.finish();
+                if (t.graphEligible(target[i]) && t.beginGraphChunk())
+                    launched[i] = 1;
+                continue;
+            }
+            const int stop = std::min(target[i], t.iteration + TrainerImpl::kGraphSteps);
+            while (t.iteration < stop && !t.graphEligible(target[i]))
+                t.step();
+        }
+        for (size_t i = 0; i < S; ++i)
+            if (launched[i]) {
+                U3DG_CUDA(cudaSetDevice(trainers[i]->device));
+                trainers[i]->endGraphChunk();
+            }
+        if (!any)
+            break;
+    }
+    for (TrainerImpl *t : trainers) {
+        U3DG_CUDA(cudaSetDevice(t->device));
+        t->finish();
+    }
+}
+
+int autotuneTileSize(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
+                     const u3dg_train_options &opt, float *msPerStep)
+{
+    static const int kTiles[3] = {16, 8, 32};
+    int best = opt.raster.tile_size;
+    float bestMs = 0.0f;
+    for (int tile : kTiles) {
+        u3dg_train_options o = opt;
+        o.raster.tile_size = tile;
+        o.iterations = std::max(o.iterations, 64);
+        TrainerImpl t(initial, imgs, count, extent, o);
+        t.stepTo(3 + TrainerImpl::kGraphSteps); // warm-up, including the first graph capture
+        t.finish();
+        cudaEvent_t a, b;
+        U3DG_CUDA(cudaEventCreate(&a));
+        U3DG_CUDA(cudaEventCreate(&b));
+        U3DG_CUDA(cudaEventRecord(a, t.stream));
+        t.stepTo(t.iteration + 2 * TrainerImpl::kGraphSteps);
+        t.finish();
+        U3DG_CUDA(cudaEventRecord(b, t.stream));
+        U3DG_CUDA(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        U3DG_CUDA(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        ms /= float(2 * TrainerImpl::kGraphSteps);
+        if (bestMs == 0.0f || ms < bestMs) {
+            bestMs = ms;
+            best = tile;
+        }
+    }
+    if (msPerStep)
+        *msPerStep = bestMs;
+    return best;
 }
 
 DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng)

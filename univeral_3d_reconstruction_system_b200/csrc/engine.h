@@ -4,6 +4,7 @@
 #include "kernels.h"
 
 #include <cstdio>
+#include <memory>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -58,6 +59,11 @@ int guardedCall(F &&f)
             throw ::u3dg::CudaError(e_, #x, __FILE__, __LINE__);       \
     } while (0)
 
+// Counts device and pinned allocations in this process. A captured CUDA graph bakes buffer addresses
+// into its nodes; it is reused only while this count is unchanged since its capture.
+unsigned long long allocEpoch();
+void bumpAllocEpoch();
+
 // Device array with capacity growth (cudaMalloc only when it has to grow).
 template <class T>
 struct DevBuf {
@@ -69,8 +75,10 @@ struct DevBuf {
     ~DevBuf() { release(); }
     void release()
     {
-        if (p)
+        if (p) {
             cudaFree(p);
+            bumpAllocEpoch();
+        }
         p = nullptr;
         cap = 0;
     }
@@ -91,6 +99,7 @@ struct DevBuf {
                                                 cudaGetErrorString(e));
         }
         cap = c;
+        bumpAllocEpoch();
     }
 };
 
@@ -113,10 +122,12 @@ struct HostPinned {
         p = nullptr;
         U3DG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&p), std::max<size_t>(n, 1) * sizeof(T)));
         cap = std::max<size_t>(n, 1);
+        bumpAllocEpoch();
     }
 };
 
 unsigned long long launchCount();
+void addLaunches(long long k);
 void checkSettings(const u3dg_raster_settings &st);
 // Uploads a host model into the params slot of an arena of capacity `cap`.
 void copyModelToArena(float *base, size_t cap, const u3dg_model &m, cudaStream_t s);
@@ -155,11 +166,12 @@ struct RasterWorkspace {
     void reserveIntersections(size_t capacity);
     // Clears the overflow / abort record (stream-ordered).
     void clearCounts(cudaStream_t stream);
+    // desc (may be null): the camera of a graph-captured step (see StepDesc).
     void project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
-                 int shDegree, cudaStream_t stream);
+                 int shDegree, cudaStream_t stream, const StepDesc *desc = nullptr);
     // Depth sort + tile binning from depthKey / rect / radius. Never waits for the device: an overflow of
     // the intersection buffers is recorded in `counts` (tagged with `iteration`) and bins nothing.
-    void bin(cudaStream_t stream, int iteration);
+    void bin(cudaStream_t stream, int iteration, const StepDesc *desc = nullptr);
     void composite(cudaStream_t stream);
     void forward(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s, const float *shRest,
                  int shDegree, cudaStream_t stream, int iteration)
@@ -212,6 +224,32 @@ struct HostSnapshot {
     std::mt19937 rng;
     int adamStep = 0;
     bool opacityWasReset = false;
+};
+
+// The host-side values of one step (what StepDesc carries to a graph-captured step).
+struct StepValues {
+    size_t view = 0;
+    StepDesc d{};
+};
+
+// A CUDA graph of kGraphSteps consecutive training steps, and what it was captured for.
+struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long epoch = 0;
+    long long kernels = 0; // kernel nodes per launch
+    int n = -1, cur = -1, icap = -1;
+    void reset()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        n = cur = icap = -1;
+    }
+    ~StepGraph() { reset(); }
 };
 
 // A queued step whose device-side status has not been checked yet.
@@ -268,6 +306,18 @@ struct TrainerImpl {
     bool profiling = false;
     PhaseTimer *timer = nullptr;
 
+    // Graph execution of runs of steps without densification, opacity reset or profiling, when every
+    // view has the same size: kGraphSteps steps per launch, their values in descriptors on the device.
+    static constexpr int kGraphSteps = 10;
+    bool useGraphs = true;
+    bool uniformViews = false;
+    StepGraph stepGraph;
+    DevBuf<StepDesc> descDev;
+    HostPinned<StepDesc> descHost;
+    HostPinned<BinCounts> graphStatus;
+    long long graphChunks = 0;        // graph launches so far
+    long long normalSteps = 0;        // steps launched one by one (the first step is never a graph)
+
     TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int count, float sceneExtent,
                 const u3dg_train_options &opt);
     ~TrainerImpl();
@@ -295,6 +345,24 @@ private:
     HostSnapshot snapshot() const;
     void restore(const HostSnapshot &s);
     void enqueueStep();
+    // Advances the host state by one step (view order, learning rates, Adam step) and returns its values.
+    StepValues nextStep();
+    // Queues the device work of one step; desc (may be null) is where graph-captured kernels read the values.
+    void launchStep(const StepValues &sv, const StepDesc *desc, BinCounts *statusDst);
+public:
+    // Whether the next kGraphSteps steps can run as one graph launch.
+    bool graphEligible(int target) const;
+    // Runs kGraphSteps steps through the step graph (capturing it when stale). Returns false after an
+    // overflow (the state is rolled back to the overflowed step, as checkOldest does).
+    bool runGraphChunk();
+    // runGraphChunk in two halves, so several trainers can have a chunk in flight at once: begin
+    // advances the host state, captures the graph if stale and launches it (no wait; false when a
+    // capture had to be discarded, with the state restored); end waits and checks the statuses.
+    bool beginGraphChunk();
+    bool endGraphChunk();
+
+private:
+    std::vector<HostSnapshot> pendingSnaps; // host state before each step of the chunk in flight
     // Checks the oldest queued step; returns false (after rolling back) when it had overflowed.
     bool checkOldest();
 };
@@ -306,4 +374,21 @@ struct DensifyResult {
 };
 DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng);
 
+// Steps every trainer by `count` iterations (or to its end), interleaving them on their own streams:
+// each round launches a graph chunk (or up to kGraphSteps single steps) per trainer before waiting
+// for any, so small scenes run concurrently on the GPU.
+void stepBatch(const std::vector<TrainerImpl *> &trainers, int count);
+
+// Tile size (8, 16 or 32) with the shortest step time for a scene, timed on throwaway trainers
+// started from the same model (the batch depth of the compositing kernels follows the tile size:
+// one staged Gaussian per thread, tile^2 / 2 threads per 16x16 or 8x8 block).
+int autotuneTileSize(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
+                     const u3dg_train_options &opt, float *msPerStep);
+
 } // namespace u3dg
+
+// The C ABI's trainer handle (include/u3dg.h). Handles owned by a batch are borrowed by callers.
+struct u3dg_trainer {
+    std::unique_ptr<u3dg::TrainerImpl> impl;
+    bool ownedByBatch = false;
+};

@@ -51,13 +51,14 @@ __device__ float shRest(const float *coef, int degree, int ch, const float d[3])
 }
 
 // Rasterizer::project (Rasterizer.cpp:137-204) for one Gaussian per thread.
-__global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camera cam, u3dg_raster_settings st,
+__global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camera camArg, u3dg_raster_settings st,
                                                      int tilesX, int tilesY, const float *shRestCoef, int shDegree,
-                                                     float3 camPos, ProjOut out)
+                                                     float3 camPos, ProjOut out, const StepDesc *desc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    const u3dg_camera cam = desc ? desc->cam : camArg;
     const float mu[3] = {P.means[3 * i], P.means[3 * i + 1], P.means[3 * i + 2]};
     const float qr[4] = {P.quats[4 * i], P.quats[4 * i + 1], P.quats[4 * i + 2], P.quats[4 * i + 3]};
     const float ls[3] = {P.scales[3 * i], P.scales[3 * i + 1], P.scales[3 * i + 2]};
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
             for (int k = 0; k < kG2d; ++k)
                 g[k] += src[k];
         }
-        const u3dg_camera &cam = a.cam;
+        const u3dg_camera &cam = a.desc ? a.desc->cam : a.cam;
         const float dmx = g[0], dmy = g[1], dA = g[2], dB = g[3], dC = g[4];
         if (a.gradAccum != nullptr) {
             const float nx = dmx * 0.5f * float(cam.width), ny = dmy * 0.5f * float(cam.height);
@@ -299,20 +300,21 @@ __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
 
     if constexpr (kAdam) {
         const Params &M = a.m, &V = a.v;
-        const float inv = a.invSqrtBc2;
+        const float inv = a.desc ? a.desc->invSqrtBc2 : a.invSqrtBc2;
+        const float *lr = a.desc ? a.desc->stepSize : a.stepSize;
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            adamOne(P.means[3 * i + k], M.means[3 * i + k], V.means[3 * i + k], gMeans[k], a.stepSize[0], inv);
+            adamOne(P.means[3 * i + k], M.means[3 * i + k], V.means[3 * i + k], gMeans[k], lr[0], inv);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            adamOne(P.scales[3 * i + k], M.scales[3 * i + k], V.scales[3 * i + k], gScales[k], a.stepSize[1], inv);
+            adamOne(P.scales[3 * i + k], M.scales[3 * i + k], V.scales[3 * i + k], gScales[k], lr[1], inv);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            adamOne(P.quats[4 * i + k], M.quats[4 * i + k], V.quats[4 * i + k], gQuats[k], a.stepSize[2], inv);
-        adamOne(P.opac[i], M.opac[i], V.opac[i], gOpac, a.stepSize[3], inv);
+            adamOne(P.quats[4 * i + k], M.quats[4 * i + k], V.quats[4 * i + k], gQuats[k], lr[2], inv);
+        adamOne(P.opac[i], M.opac[i], V.opac[i], gOpac, lr[3], inv);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            adamOne(P.colors[3 * i + k], M.colors[3 * i + k], V.colors[3 * i + k], gColors[k], a.stepSize[4], inv);
+            adamOne(P.colors[3 * i + k], M.colors[3 * i + k], V.colors[3 * i + k], gColors[k], lr[4], inv);
     } else {
         const Params &G = a.grads;
         if (a.radius[i] > 0) {
@@ -500,7 +502,8 @@ inline int blocks(long long n, int threads) { return int((n + threads - 1) / thr
 } // namespace
 
 void launchProject(const Params &P, int n, const u3dg_camera &cam, const u3dg_raster_settings &st, int tilesX,
-                   int tilesY, const float *shRest, int shDegree, const ProjOut &out, cudaStream_t s)
+                   int tilesY, const float *shRest, int shDegree, const ProjOut &out, cudaStream_t s,
+                   const StepDesc *desc)
 {
     if (n <= 0)
         return;
@@ -511,7 +514,9 @@ void launchProject(const Params &P, int n, const u3dg_camera &cam, const u3dg_ra
         camPos.y = -(cam.R[1] * cam.t[0] + cam.R[4] * cam.t[1] + cam.R[7] * cam.t[2]);
         camPos.z = -(cam.R[2] * cam.t[0] + cam.R[5] * cam.t[1] + cam.R[8] * cam.t[2]);
     }
-    { projectKernel<<<blocks(n, 256), 256, 0, s>>>(P, n, cam, st, tilesX, tilesY, shRest, shDegree, camPos, out); countLaunch(); }
+    if (desc)
+        shDegree = 0;
+    { projectKernel<<<blocks(n, 256), 256, 0, s>>>(P, n, cam, st, tilesX, tilesY, shRest, shDegree, camPos, out, desc); countLaunch(); }
 }
 
 void launchChain(const ChainArgs &a, bool adam, cudaStream_t s)

@@ -16,6 +16,18 @@ struct BinCounts {
     int pad[3];
 };
 
+// The values of one training step that change from step to step (view, target image, iteration,
+// Adam step sizes). Launches given a StepDesc read them from device memory instead of their by-value
+// arguments, so a captured CUDA graph of training steps serves any views and learning rates.
+struct StepDesc {
+    u3dg_camera cam;
+    const uint8_t *target; // the view's uint8 image
+    int iteration;         // iteration count before the step (0-based step index)
+    float stepSize[5];     // Adam: lr / bc1 per group
+    float invSqrtBc2;
+    int pad[2];
+};
+
 // Outputs of the projection kernel, one entry per Gaussian.
 struct ProjOut {
     SplatRec *rec;      // raster record (valid where radius > 0)
@@ -46,11 +58,14 @@ struct ChainArgs {
     Params m, v;          // Adam mode: moments
     float stepSize[5];    // Adam mode: lr / bc1 per group
     float invSqrtBc2;
+    const StepDesc *desc; // when set: cam, stepSize and invSqrtBc2 come from here
 };
 
 // gaussian.cu
+// desc (may be null): the camera comes from desc->cam (no spherical harmonics in that mode).
 void launchProject(const Params &P, int n, const u3dg_camera &cam, const u3dg_raster_settings &st, int tilesX,
-                   int tilesY, const float *shRest, int shDegree, const ProjOut &out, cudaStream_t s);
+                   int tilesY, const float *shRest, int shDegree, const ProjOut &out, cudaStream_t s,
+                   const StepDesc *desc = nullptr);
 void launchChain(const ChainArgs &a, bool adam, cudaStream_t s);
 void launchAdamSegment(float *p, const float *g, float *m, float *v, int len, float stepSize, float invSqrtBc2,
                        cudaStream_t s);
@@ -83,7 +98,8 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
 void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt, int *rankOf,
                       cudaStream_t s);
 // Sets counts->n and checks *total against the intersection capacity (see BinCounts).
-void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s);
+void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
+                         const StepDesc *desc = nullptr);
 void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 // Emission of the intersections in depth-rank order: tile key and Gaussian id per intersection.
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
@@ -115,13 +131,16 @@ struct LossScratch {
 };
 int lossBlocks(int width, int height);
 // target is either float (targetF) or uint8 (targetU8, converted as float(u8) * (1/255f)).
+// desc (may be null): the uint8 target comes from desc->target.
 void launchLoss(const float *render, const float *targetF, const uint8_t *targetU8, int width, int height, float lambda,
-                float *grad, const LossScratch &ls, cudaStream_t s);
+                float *grad, const LossScratch &ls, cudaStream_t s, const StepDesc *desc = nullptr);
 // Reduces the block sums into the step's LossValue / PSNR and updates the EMA stats
 // (Trainer.cpp:88-92) unless counts (may be null) records an aborted step. out3 (may be null) gets
 // total, l1, ssim; psnrOut (may be null) the PSNR.
+// desc (may be null): iteration is desc->iteration + 1.
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
-                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s);
+                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s,
+                        const StepDesc *desc = nullptr);
 // PSNR of the render against a uint8 target, accumulated in double (evaluatePsnr).
 void launchPsnrU8(const float *render, const uint8_t *target, size_t count, double *sumOut, cudaStream_t s);
 void launchPsnrF(const float *a, const float *b, size_t count, double *sumOut, cudaStream_t s);

@@ -61,8 +61,11 @@ __device__ __forceinline__ double blockSumDouble(double v)
 
 __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *render, const float *targetF,
                                                               const uint8_t *targetU8, int W, int H, float lambda,
-                                                              float *grad, float *abc, double *blockSums)
+                                                              float *grad, float *abc, double *blockSums,
+                                                              const StepDesc *desc)
 {
+    if (desc)
+        targetU8 = desc->target;
     __shared__ float sx[kIH][kIW], sy[kIH][kIW];
     __shared__ float hm[5][kIH][kTW];
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
@@ -162,8 +165,10 @@ __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *rende
 
 __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *render, const float *targetF,
                                                                const uint8_t *targetU8, int W, int H, const float *abc,
-                                                               float *grad)
+                                                               float *grad, const StepDesc *desc)
 {
+    if (desc)
+        targetU8 = desc->target;
     __shared__ float sm[3][kIH][kIW];
     __shared__ float hm[3][kIH][kTW];
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
@@ -221,8 +226,11 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
 // Single block: fixed-order sum of the block partials, LossValue, PSNR and the EMA stats.
 __global__ void __launch_bounds__(kThreads) lossFinalizeKernel(const double *blockSums, int blocks, int W, int H,
                                                                float lambda, DevStats *stats, int iteration,
-                                                               const BinCounts *counts, float *out3, float *psnrOut)
+                                                               const BinCounts *counts, float *out3, float *psnrOut,
+                                                               const StepDesc *desc)
 {
+    if (desc)
+        iteration = desc->iteration + 1;
     if (counts != nullptr && counts->abortIter >= 0)
         stats = nullptr; // an aborted step leaves the statistics alone (it is replayed)
     double s0 = 0, s1 = 0, s2 = 0;
@@ -328,21 +336,21 @@ constexpr int kSqBlocks = 296; // 2 x 148 SMs
 int lossBlocks(int width, int height) { return ((width + kTW - 1) / kTW) * ((height + kTH - 1) / kTH); }
 
 void launchLoss(const float *render, const float *targetF, const uint8_t *targetU8, int width, int height, float lambda,
-                float *grad, const LossScratch &ls, cudaStream_t s)
+                float *grad, const LossScratch &ls, cudaStream_t s, const StepDesc *desc)
 {
     ensureWindow();
     dim3 g((width + kTW - 1) / kTW, (height + kTH - 1) / kTH);
     { lossForwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, lambda, grad, ls.abc,
-                                             ls.blockSums); countLaunch(); }
+                                             ls.blockSums, desc); countLaunch(); }
     if (lambda > 0.0f)
-        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad); countLaunch(); }
+        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad, desc); countLaunch(); }
 }
 
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
-                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s)
+                        const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s, const StepDesc *desc)
 {
     { lossFinalizeKernel<<<1, kThreads, 0, s>>>(ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
-                                              counts, out3, psnrOut); countLaunch(); }
+                                              counts, out3, psnrOut, desc); countLaunch(); }
 }
 
 void launchPsnrU8(const float *render, const uint8_t *target, size_t count, double *sumOut, cudaStream_t s)

@@ -19,6 +19,7 @@ u3dg_render_sh, or the CPU oracle in tests), so it is a separate step (`render_t
 """
 from __future__ import annotations
 
+import dataclasses
 import math
 from dataclasses import dataclass, field
 
@@ -56,6 +57,23 @@ PRESETS = {
     "tiny": SceneSpec("tiny", 2_000, 8, 96, 72, 90.0, "ring", 600, 300, 4_000),
     "small": SceneSpec("small", 8_000, 12, 160, 120, 150.0, "ring", 2_000, 600, 12_000),
 }
+
+
+def batched_specs(seed: int = 0, count: int = 16) -> list:
+    """The batched multi-scene workload: `count` scenes with ground-truth counts log-uniform in
+    [20k, 300k], view counts uniform in [30, 200] and widths drawn from {320, 480, 640}; each scene
+    otherwise follows the preset of its width (Fast / Balanced / High: focal length, camera layout,
+    initial points, schedule and Gaussian cap 80k / 150k / 300k)."""
+    rng = np.random.default_rng([seed, 3])
+    by_width = {320: "fast", 480: "balanced", 640: "high"}
+    specs = []
+    for k in range(count):
+        gt = int(round(math.exp(rng.uniform(math.log(20e3), math.log(300e3)))))
+        views = int(rng.integers(30, 201))
+        width = int(rng.choice(sorted(by_width)))
+        base = PRESETS[by_width[width]]
+        specs.append(dataclasses.replace(base, name=f"batch{k}-{base.name}", gt_count=gt, views=views))
+    return specs
 
 
 @dataclass

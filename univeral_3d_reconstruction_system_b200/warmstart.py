@@ -52,6 +52,8 @@ LABEL_ITERATIONS = 3000
 TRAIN_SEEDS = tuple(range(100, 164))  # 64 label scenes
 EVAL_SEEDS = tuple(range(1000, 1008))  # 8 held-out scenes
 OPACITY_CLIP = 6.0
+# The training loss's default output weights (warmstart_host.cu): log-scales, quaternion, opacity, colour.
+LOSS_WEIGHTS = np.array([1, 1, 1, 0.5, 0.5, 0.5, 0.5, 0.25, 1, 1, 1], np.float64)
 
 
 # ------------------------------------------------------------------ scenes
@@ -316,13 +318,16 @@ def main(argv=None) -> int:
         meta = {"label_iterations": a.label_iterations, "train_seeds": list(TRAIN_SEEDS[:a.scenes]),
                 "rows": int(len(X)), "epoch_losses": losses, "train_seconds": round(train_s, 2)}
         hold = []
+        net = api.WarmStartNet(params)
         for seed in EVAL_SEEDS[:a.holdout_labels]:
             sc = build_scene(seed)
             Xh, Th, base = label_scene(sc, a.label_iterations)
+            mse_net = np.mean((net.forward(Xh).astype(np.float64) - Th) ** 2, axis=0)
+            mse_plain = np.mean((plain_targets(base).astype(np.float64) - Th) ** 2, axis=0)
             hold.append({"seed": seed, "network_label_loss": label_loss(params, Xh, Th),
-                         "plain_label_loss": float(np.sum(
-                             np.array([1, 1, 1, .5, .5, .5, .5, .25, 1, 1, 1]) *
-                             np.mean((plain_targets(base).astype(np.float64) - Th) ** 2, axis=0)) / 11.0)})
+                         "plain_label_loss": float(np.sum(LOSS_WEIGHTS * mse_plain) / 11.0),
+                         "per_output_mse_network": [round(float(v), 5) for v in mse_net],
+                         "per_output_mse_plain": [round(float(v), 5) for v in mse_plain]})
             log(f"held-out labels seed {seed}: {hold[-1]}")
         meta["holdout_label_loss"] = hold
         save(a.out, params, meta)
