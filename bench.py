@@ -299,22 +299,24 @@ def run_ours(args, dist: Dist) -> dict:
     if args.warmstart and dist.world == 1:
         res["warmstart"] = run_warmstart(args)
     if args.batched:
-        res["batched"] = run_batched(args)
+        res["batched"] = run_batched(args, dist)
     return res
 
 
-def run_batched(args) -> dict:
+def run_batched(args, dist: Dist) -> dict:
     """Batched multi-scene training: 16 seeded scenes (scenes.batched_specs) trained together by one
     u3dg_batch (per-scene streams, step graphs, tile sizes from the autotuner), then each scene alone
-    with its tuned tile size. Reports the aggregate iterations/s of both and every scene's PSNR."""
+    with its tuned tile size. Reports the aggregate iterations/s of both and every scene's PSNR. With
+    N ranks, rank r takes scenes r, r + N, ... (scenes are independent: no collective on the data
+    path); the rates are total iterations over the slowest rank's time."""
     from univeral_3d_reconstruction_system_b200 import api
     from univeral_3d_reconstruction_system_b200.scenes import batched_specs, make_scene
     from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
 
     t0 = time.time()
-    scenes, specs = [], batched_specs(0, 16)
+    scenes, specs = [], [sp for k, sp in enumerate(batched_specs(0, 16)) if k % dist.world == dist.rank]
     for k, sp in enumerate(specs):
-        sc = make_scene(sp, 500 + k)
+        sc = make_scene(sp, 500 + k * dist.world + dist.rank)
         imgs = api.renderViewsSh(sc.truth, sc.sh_rest, 3, sc.cameras, RasterSettings())
         sc.images = [TrainImage(c, im) for c, im in zip(sc.cameras, imgs)]
         opt = sc.options()
@@ -344,10 +346,20 @@ def run_batched(args) -> dict:
         t.close()
     b.close()
     diffs = [abs(r["psnr_batched"] - r["psnr_alone"]) for r in rows]
-    out = {"scenes": 16, "iterations_total": total, "batched_ms": round(ms, 2),
-           "batched_it_per_s": round(total / (ms * 1e-3), 1), "sequential_ms": round(seq_ms, 2),
-           "sequential_it_per_s": round(total / (seq_ms * 1e-3), 1), "speedup": round(seq_ms / ms, 3),
-           "autotune_s": round(tune_s, 2), "max_psnr_diff_db": round(max(diffs), 5), "per_scene": rows}
+    total_all = total
+    if dist.world > 1:
+        import torch
+        dev = f"cuda:{dist.local}" if dist.backend == "nccl" else "cpu"
+        tot = torch.tensor([float(total)], dtype=torch.float64, device=dev)
+        dist.pg.all_reduce(tot, op=dist.pg.ReduceOp.SUM)
+        total_all = int(tot.item())
+        ms, seq_ms = dist.max(ms), dist.max(seq_ms)
+        diffs.append(dist.max(max(diffs)))
+    out = {"scenes": 16, "ranks": dist.world, "iterations_total": total_all, "batched_ms": round(ms, 2),
+           "batched_it_per_s": round(total_all / (ms * 1e-3), 1), "sequential_ms": round(seq_ms, 2),
+           "sequential_it_per_s": round(total_all / (seq_ms * 1e-3), 1), "speedup": round(seq_ms / ms, 3),
+           "autotune_s": round(tune_s, 2), "max_psnr_diff_db": round(max(diffs), 5),
+           "per_scene": rows if dist.world == 1 else f"rank 0 scenes: {rows}"}
     log(f"batched: {out['batched_it_per_s']} it/s vs sequential {out['sequential_it_per_s']} it/s, "
         f"max PSNR diff {out['max_psnr_diff_db']} dB")
     return out

@@ -14,6 +14,7 @@
 
 #include <cstdint>
 #include <stdexcept>
+#include <cstdio>
 #include <string>
 #include <utility>
 #include <vector>
@@ -339,6 +340,134 @@ inline float psnr(const float *a, const float *b, std::size_t count)
     check(u3dg_psnr(a, b, count, &p));
     return p;
 }
+
+// ------------------------------------------------------------------ learned warm-start (no reference counterpart)
+
+// The warm-start network (134 -> 128 -> 128 -> 128 -> 11). fromFile reads the 51,723 little-endian
+// float32 parameters the package ships (data/warmstart_high.f32).
+class WarmStartNet
+{
+public:
+    explicit WarmStartNet(const std::vector<float> &params)
+    {
+        if (params.size() != std::size_t(U3DG_MLP_PARAMS))
+            throw Error(U3DG_ERR_INVALID_ARG, "warm-start network needs 51723 parameters");
+        check(u3dg_mlp_create(params.data(), 0, &m_h));
+    }
+    static WarmStartNet fromFile(const std::string &path)
+    {
+        std::vector<float> p(U3DG_MLP_PARAMS);
+        std::FILE *f = std::fopen(path.c_str(), "rb");
+        if (!f)
+            throw Error(U3DG_ERR_IO, "cannot open " + path);
+        const std::size_t got = std::fread(p.data(), sizeof(float), p.size(), f);
+        std::fclose(f);
+        if (got != p.size())
+            throw Error(U3DG_ERR_IO, path + " is not a warm-start parameter file");
+        return WarmStartNet(p);
+    }
+    WarmStartNet(WarmStartNet &&o) noexcept : m_h(o.m_h) { o.m_h = nullptr; }
+    WarmStartNet(const WarmStartNet &) = delete;
+    WarmStartNet &operator=(const WarmStartNet &) = delete;
+    ~WarmStartNet() { u3dg_mlp_destroy(m_h); }
+    u3dg_mlp *handle() const { return m_h; }
+
+private:
+    u3dg_mlp *m_h = nullptr;
+};
+
+// initGaussiansFromPoints refined by the network from the points' neighbourhoods and the training
+// views; net == nullptr gives initGaussiansFromPoints exactly.
+inline GaussianModel warmStartFromPoints(const WarmStartNet *net, const std::vector<float> &xyz,
+                                         const std::vector<float> &rgb, const std::vector<TrainImage> &images)
+{
+    GaussianModel m;
+    const std::size_t n = xyz.size() / 3;
+    m.resize(n);
+    std::vector<u3dg_image> views(images.size());
+    for (std::size_t k = 0; k < images.size(); ++k)
+        views[k] = {images[k].camera, images[k].rgb.data()};
+    u3dg_model v = m.view();
+    check(u3dg_warmstart_init(net ? net->handle() : nullptr, xyz.data(), rgb.size() >= n * 3 ? rgb.data() : nullptr,
+                              n, views.data(), int(views.size()), &v));
+    return m;
+}
+
+// ------------------------------------------------------------------ batched training (no reference counterpart)
+
+// Several scenes trained at once on the current device; scene(k) gives the per-scene queries.
+class BatchTrainer
+{
+public:
+    struct Scene {
+        GaussianModel initial;
+        std::vector<TrainImage> images;
+        float sceneExtent = 1.0f;
+        TrainOptions options;
+    };
+    explicit BatchTrainer(std::vector<Scene> scenes, bool autotune = true) : m_scenes(std::move(scenes))
+    {
+        const std::size_t S = m_scenes.size();
+        std::vector<u3dg_model> models(S);
+        std::vector<std::vector<u3dg_image>> views(S);
+        std::vector<const u3dg_image *> viewPtrs(S);
+        std::vector<int> counts(S);
+        std::vector<float> extents(S);
+        std::vector<u3dg_train_options> opts(S);
+        for (std::size_t s = 0; s < S; ++s) {
+            models[s] = m_scenes[s].initial.view();
+            for (const TrainImage &i : m_scenes[s].images)
+                views[s].push_back({i.camera, i.rgb.data()});
+            viewPtrs[s] = views[s].data();
+            counts[s] = int(views[s].size());
+            extents[s] = m_scenes[s].sceneExtent;
+            opts[s] = m_scenes[s].options;
+        }
+        check(u3dg_batch_create(models.data(), viewPtrs.data(), counts.data(), extents.data(), opts.data(), int(S),
+                                autotune ? 1 : 0, &m_b));
+    }
+    ~BatchTrainer() { u3dg_batch_destroy(m_b); }
+    BatchTrainer(const BatchTrainer &) = delete;
+    BatchTrainer &operator=(const BatchTrainer &) = delete;
+
+    // Every scene advances by `count` iterations (or to the end of its schedule).
+    void step(int count = 1) { check(u3dg_batch_step(m_b, count)); }
+    std::size_t size() const { return m_scenes.size(); }
+    int tileSize(int scene) const
+    {
+        int t = 0;
+        check(u3dg_batch_tile_size(m_b, scene, &t, nullptr));
+        return t;
+    }
+    // The scene's model, copied back from the GPU.
+    GaussianModel model(int scene) const
+    {
+        u3dg_trainer *t = trainer(scene);
+        std::size_t n = 0;
+        check(u3dg_trainer_size(t, &n));
+        GaussianModel m;
+        m.resize(n);
+        u3dg_model v = m.view();
+        check(u3dg_trainer_download(t, &v, n, &n));
+        return m;
+    }
+    float evaluatePsnr(int scene)
+    {
+        float p = 0;
+        check(u3dg_trainer_eval_psnr(trainer(scene), &p));
+        return p;
+    }
+
+private:
+    u3dg_trainer *trainer(int scene) const
+    {
+        u3dg_trainer *t = nullptr;
+        check(u3dg_batch_trainer(m_b, scene, &t));
+        return t;
+    }
+    std::vector<Scene> m_scenes;
+    u3dg_batch *m_b = nullptr;
+};
 
 } // namespace gpu
 } // namespace u3d

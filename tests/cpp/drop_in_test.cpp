@@ -122,6 +122,32 @@ int main()
     std::vector<float> img;
     trainer.render(images[0].camera, img);
     EXPECT(img.size() == std::size_t(96 * 72 * 3));
+
+    // The learned warm-start without a network is initGaussiansFromPoints exactly.
+    std::vector<u3d::gpu::TrainImage> gpuImages;
+    for (const u3d::TrainImage &i : images)
+        gpuImages.push_back(u3d::gpu::imageFrom(i));
+    const u3d::gpu::GaussianModel plain = u3d::gpu::warmStartFromPoints(nullptr, xyz, rgb, gpuImages);
+    const u3d::gpu::GaussianModel ref = u3d::gpu::modelFrom(init);
+    EXPECT(plain.means == ref.means && plain.scales == ref.scales && plain.quats == ref.quats &&
+           plain.opacities == ref.opacities && plain.colors == ref.colors);
+
+    // Two copies of the scene trained as one batch end where the single trainer ended.
+    std::vector<u3d::gpu::BatchTrainer::Scene> scenes(2);
+    for (auto &sc : scenes) {
+        sc.initial = ref;
+        sc.images = gpuImages;
+        sc.sceneExtent = 4.4f;
+        sc.options = u3d::gpu::optionsFrom(opt);
+    }
+    u3d::gpu::BatchTrainer batch(std::move(scenes), false);
+    batch.step(1500);
+    const u3d::gpu::GaussianModel single = u3d::gpu::modelFrom(out);
+    for (int s = 0; s < 2; ++s) {
+        const u3d::gpu::GaussianModel m = batch.model(s);
+        EXPECT(m.means == single.means && m.opacities == single.opacities && m.colors == single.colors);
+        EXPECT(std::fabs(batch.evaluatePsnr(s) - after) < 1e-6f);
+    }
     if (failures == 0)
         std::printf("drop-in ok\n");
     return failures == 0 ? 0 : 1;

@@ -381,7 +381,8 @@ void stepBatch(const std::vector<TrainerImpl *> &trainers, int count);
 
 // Tile size (8, 16 or 32) with the shortest step time for a scene, timed on throwaway trainers
 // started from the same model (the batch depth of the compositing kernels follows the tile size:
-// one staged Gaussian per thread, tile^2 / 2 threads per 16x16 or 8x8 block).
+// one staged Gaussian per thread, tile^2 / 2 threads per 16x16 or 8x8 block). Tile 32, whose
+// partial gradients are added atomically, must be at least 3% faster than the best of 8 and 16.
 int autotuneTileSize(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
                      const u3dg_train_options &opt, float *msPerStep);
 

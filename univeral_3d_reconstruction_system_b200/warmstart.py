@@ -47,7 +47,9 @@ from .schedule import run_schedule
 from .types import GaussianModel, RasterSettings, TrainImage, TrainOptions
 
 DATA_DIR = Path(__file__).resolve().parent / "data"
-WEIGHTS_PATH = DATA_DIR / "warmstart_high.npz"
+# 51,723 little-endian float32 parameters (per layer W then b), readable from C/C++ with one fread;
+# the training record (seeds, losses, held-out label losses) sits beside it as <name>.json.
+WEIGHTS_PATH = DATA_DIR / "warmstart_high.f32"
 LABEL_ITERATIONS = 3000
 TRAIN_SEEDS = tuple(range(100, 164))  # 64 label scenes
 EVAL_SEEDS = tuple(range(1000, 1008))  # 8 held-out scenes
@@ -219,13 +221,20 @@ def label_loss(params, X, T) -> float:
 
 
 def save(path: Path, params: np.ndarray, meta: dict) -> None:
+    path = Path(path)
     path.parent.mkdir(parents=True, exist_ok=True)
-    np.savez(path, params=params.astype(np.float32), meta=json.dumps(meta))
+    np.asarray(params, "<f4").reshape(-1).tofile(path)
+    path.with_suffix(".json").write_text(json.dumps(meta, indent=1))
 
 
 def load_params(path: Path = WEIGHTS_PATH):
-    with np.load(path) as z:
-        return z["params"].astype(np.float32), json.loads(str(z["meta"]))
+    path = Path(path)
+    params = np.fromfile(path, "<f4").astype(np.float32)
+    if params.size != api.MLP_PARAMS:
+        raise ValueError(f"{path}: {params.size} parameters, expected {api.MLP_PARAMS}")
+    meta_path = path.with_suffix(".json")
+    meta = json.loads(meta_path.read_text()) if meta_path.exists() else {}
+    return params, meta
 
 
 def load_network(path: Path = WEIGHTS_PATH) -> api.WarmStartNet:
