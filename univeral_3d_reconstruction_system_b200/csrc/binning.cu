@@ -267,28 +267,51 @@ __global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int
     c->effTotal = (over || c->abortIter >= 0) ? 0 : t;
 }
 
-// One thread per intersection (grid-stride): binary search of its rank in offs, then its tile in the
+// One warp per 32 consecutive depth ranks (grid-stride): the warp writes its ranks' intersections in
+// order, 32 at a time. Each lane finds the rank of its intersection as the last of the warp's 32 start
+// offsets not above it (a binary search over lanes with shuffles; empty ranks share their start with
+// the next rank, so the search lands on the rank that owns the slot), then its tile in that rank's
 // rectangle (row-major, as the reference's ty/tx loops).
-__global__ void emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c,
-                           int tilesX, uint32_t *keys, int *emitGid)
+__global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n,
+                                                  const BinCounts *c, int tilesX, uint32_t *keys, int *emitGid)
 {
     const int total = c->effTotal;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-        int lo = 0, hi = n; // last r with offs[r] <= e
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (offs[mid] <= e)
-                lo = mid;
-            else
-                hi = mid;
+    if (total <= 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int warps = int((gridDim.x * blockDim.x) >> 5);
+    for (int w = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w * 32 < n; w += warps) {
+        const int r = w * 32 + lane;
+        const bool valid = r < n;
+        const int o = valid ? offs[r] : INT_MAX;
+        int g = 0;
+        int4 q = make_int4(0, 0, 1, 1);
+        if (valid) {
+            g = int(sortedIds[r]);
+            q = rect[g];
         }
-        const int g = int(sortedIds[lo]);
-        const int4 q = rect[g];
-        const int k = e - offs[lo];
-        const int w = q.z - q.x;
-        const int ty = q.y + k / w, tx = q.x + k % w;
-        keys[e] = uint32_t(ty * tilesX + tx);
-        emitGid[e] = g;
+        const int first = offs[w * 32], last = min(offs[min(w * 32 + 32, n)], total);
+        for (int e0 = first; e0 < last; e0 += 32) {
+            const int e = e0 + lane;
+            int l = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int oc = __shfl_sync(0xffffffffu, o, l + step);
+                if (oc <= e)
+                    l += step;
+            }
+            const int ol = __shfl_sync(0xffffffffu, o, l);
+            const int gl = __shfl_sync(0xffffffffu, g, l);
+            const int qx = __shfl_sync(0xffffffffu, q.x, l), qy = __shfl_sync(0xffffffffu, q.y, l);
+            const int qz = __shfl_sync(0xffffffffu, q.z, l);
+            if (e < last) {
+                const int k = e - ol;
+                const int wdt = qz - qx;
+                const int ty = qy + k / wdt, tx = qx + k % wdt;
+                keys[e] = uint32_t(ty * tilesX + tx);
+                emitGid[e] = gl;
+            }
+        }
     }
 }
 
@@ -384,7 +407,7 @@ void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, in
                 int tilesX, uint32_t *keys, int *emitGid, cudaStream_t s)
 {
     if (n > 0 && capacity > 0)
-        { emitKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, keys, emitGid); countLaunch(); }
+        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, keys, emitGid); countLaunch(); }
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,

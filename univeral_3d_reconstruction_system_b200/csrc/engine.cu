@@ -69,6 +69,9 @@ RasterWorkspace::RasterWorkspace()
     c.abortIter = -1;
     *hostCounts.p = c;
     U3DG_CUDA(cudaMemcpy(counts.p, &c, sizeof(c), cudaMemcpyHostToDevice));
+    // The compositing kernels' block counters start at zero and are reset by each launch's last CTA.
+    blockCounters.reserve(4, true);
+    U3DG_CUDA(cudaMemset(blockCounters.p, 0, 4 * sizeof(int)));
 }
 
 void RasterWorkspace::clearCounts(cudaStream_t stream)
@@ -187,6 +190,11 @@ RasterArgs RasterWorkspace::rasterArgs() const
         a.bg[k] = st.background[k];
     a.minAlpha = st.min_alpha;
     a.minTransmittance = st.min_transmittance;
+    const int pb = st.tile_size <= 8 ? 8 : 16;
+    a.blocksX = (cam.width + pb - 1) / pb;
+    a.blocksY = (cam.height + pb - 1) / pb;
+    a.blockOrder = blockOrder.p;
+    a.counters = blockCounters.p;
     return a;
 }
 
@@ -196,7 +204,11 @@ void RasterWorkspace::composite(cudaStream_t stream)
     rgb.reserve(P * 3);
     finalT.reserve(P);
     nContrib.reserve(P);
-    launchCompositeForward(rasterArgs(), rgb.p, finalT.p, nContrib.p, stream);
+    const int pb = st.tile_size <= 8 ? 8 : 16;
+    blockOrder.reserve(size_t(std::max(1, ((cam.width + pb - 1) / pb) * ((cam.height + pb - 1) / pb))));
+    const RasterArgs a = rasterArgs();
+    launchBlockOrder(a, blockOrder.p, stream);
+    launchCompositeForward(a, rgb.p, finalT.p, nContrib.p, stream);
 }
 
 void RasterWorkspace::backwardComposite(const float *dLdRgb, cudaStream_t stream)

@@ -151,6 +151,7 @@ struct RasterWorkspace {
     int icap = 0;
     // per tile / pixel
     DevBuf<int> tileOffsets, nContrib;
+    DevBuf<int> blockOrder, blockCounters; // compositing schedule: pixel blocks by list length, counters
     DevBuf<float> rgb, finalT;
     // device-side sizes of the last pass and their pinned host copy
     DevBuf<BinCounts> counts;

@@ -117,7 +117,14 @@ struct RasterArgs {
     int width, height, tileSize, tilesX;
     float bg[3];
     float minAlpha, minTransmittance;
+    // Persistent scheduling over the pixel blocks (PB x PB, PB = 8 for tile size 8, else 16).
+    int blocksX, blocksY;
+    const int *blockOrder; // pixel blocks, heaviest tile list first (launchBlockOrder)
+    int *counters;         // 4 ints, zero between launches: forward [0..1], backward [2..3]
 };
+// Orders the pixel blocks by the list length of their tile, longest first (log-scale buckets), into
+// order[blocksX * blocksY].
+void launchBlockOrder(const RasterArgs &a, int *order, cudaStream_t s);
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s);
 // partial: 9 floats per intersection in emission order; zeroed by the caller when tileSize > 16.
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,

@@ -12,6 +12,8 @@
 
 #include "raster_common.cuh"
 
+#include <algorithm>
+
 namespace u3dg {
 
 namespace {
@@ -44,18 +46,15 @@ __device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const fl
 }
 
 template <int PB>
-__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
-                                                                              int *nContrib)
+__device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by, float *rgb, float *finalT,
+                                             int *nContrib, float4 *sP, float4 *sQ, float4 *sR,
+                                             uint32_t (*mask)[RasterShape<PB>::NW])
 {
     using S = RasterShape<PB>;
     constexpr int NT = S::NT, NW = S::NW;
-    __shared__ float4 sP[NT]; // mx, my, ex, ey
-    __shared__ float4 sQ[NT]; // A, B, C, alpha
-    __shared__ float4 sR[NT]; // r, g, b, depth
-    __shared__ uint32_t mask[NW][NW];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const WarpBlock<PB> wb(warp, lane);
-    const int tile = tileOf<PB>(a);
+    const WarpBlock<PB> wb(warp, lane, bx, by);
+    const int tile = tileOf<PB>(a, bx, by);
     const int start = a.tileOffsets[tile], end = a.tileOffsets[tile + 1];
     const bool in0 = wb.px < a.width && wb.py0 < a.height, in1 = wb.px < a.width && wb.py1 < a.height;
     bool done0 = !in0, done1 = !in1;
@@ -68,7 +67,7 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(Ra
     for (int b0 = start; b0 < end; b0 += NT) {
         if (__syncthreads_count(done0 && done1) == NT)
             break;
-        stage<PB>(rec, a.list, b0 + tid, b0 + tid < end, tid, sP, sQ, sR, mask);
+        stage<PB>(rec, a.list, b0 + tid, b0 + tid < end, tid, sP, sQ, sR, mask, bx, by);
         __syncthreads();
         for (int k = 0; k < NW && !(done0 && done1); ++k) {
             uint32_t bits = mask[warp][k];
@@ -105,16 +104,101 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(Ra
     }
 }
 
+template <int PB>
+__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
+                                                                              int *nContrib)
+{
+    using S = RasterShape<PB>;
+    constexpr int NT = S::NT, NW = S::NW;
+    __shared__ float4 sP[NT]; // mx, my, ex, ey
+    __shared__ float4 sQ[NT]; // A, B, C, alpha
+    __shared__ float4 sR[NT]; // r, g, b, depth
+    __shared__ uint32_t mask[NW][NW];
+    __shared__ int sNext;
+    const int units = a.blocksX * a.blocksY;
+    for (int b = nextBlock(a, a.counters, &sNext); b < units; b = nextBlock(a, a.counters, &sNext))
+        forwardBlock<PB>(a, b % a.blocksX, b / a.blocksX, rgb, finalT, nContrib, sP, sQ, sR, mask);
+}
+
+// One CTA: the pixel blocks bucketed by the list length of their tile on a log scale (four buckets
+// per power of two), longest first. The order only schedules work (every block's result is the same
+// whichever CTA computes it when), so blocks within a bucket may come in any order.
+constexpr int kOrderBuckets = 132;
+
+__device__ __forceinline__ int lengthBucket(unsigned len)
+{
+    if (len == 0)
+        return kOrderBuckets - 1;
+    const int msb = 31 - __clz(len);
+    const int sub = msb >= 2 ? int((len >> (msb - 2)) & 3u) : int((len << (2 - msb)) & 3u);
+    return kOrderBuckets - 2 - (msb * 4 + sub); // longer lists: smaller bucket index
+}
+
+__global__ void __launch_bounds__(1024) blockOrderKernel(const int *tileOffsets, int blocksX, int blocksY, int pb,
+                                                         int tileSize, int tilesX, int *order)
+{
+    __shared__ int count[kOrderBuckets];
+    __shared__ int cursor[kOrderBuckets];
+    const int units = blocksX * blocksY;
+    for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x)
+        count[b] = 0;
+    __syncthreads();
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int bx = u % blocksX, by = u / blocksX;
+        const int t = (by * pb / tileSize) * tilesX + bx * pb / tileSize;
+        atomicAdd(&count[lengthBucket(unsigned(tileOffsets[t + 1] - tileOffsets[t]))], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = 0; b < kOrderBuckets; ++b) {
+            cursor[b] = run;
+            run += count[b];
+        }
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int bx = u % blocksX, by = u / blocksX;
+        const int t = (by * pb / tileSize) * tilesX + bx * pb / tileSize;
+        const int pos = atomicAdd(&cursor[lengthBucket(unsigned(tileOffsets[t + 1] - tileOffsets[t]))], 1);
+        order[pos] = u;
+    }
+}
+
+// CTAs that can be resident at once for a kernel (cached per kernel and dynamic shared memory size).
+template <class K>
+int residentCtas(K kernel, int threads, size_t smem)
+{
+    int dev = 0, sms = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem);
+    return std::max(1, sms * std::max(1, perSm));
+}
+
 } // namespace
+
+void launchBlockOrder(const RasterArgs &a, int *order, cudaStream_t s)
+{
+    const int units = a.blocksX * a.blocksY;
+    if (units <= 0)
+        return;
+    const int pb = a.tileSize <= 8 ? 8 : 16;
+    { blockOrderKernel<<<1, 1024, 0, s>>>(a.tileOffsets, a.blocksX, a.blocksY, pb, a.tileSize, a.tilesX, order); countLaunch(); }
+}
 
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
 {
+    const int units = a.blocksX * a.blocksY;
+    if (units <= 0)
+        return;
+    const RasterArgs &f = a; // forward: counters[0..1]
     if (a.tileSize <= 8) {
-        dim3 g((a.width + 7) / 8, (a.height + 7) / 8);
-        { compositeForwardKernel<8><<<g, RasterShape<8>::NT, 0, s>>>(a, rgb, finalT, nContrib); countLaunch(); }
+        static const int ctas = residentCtas(compositeForwardKernel<8>, RasterShape<8>::NT, 0);
+        { compositeForwardKernel<8><<<std::min(units, ctas), RasterShape<8>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
     } else {
-        dim3 g((a.width + 15) / 16, (a.height + 15) / 16);
-        { compositeForwardKernel<16><<<g, RasterShape<16>::NT, 0, s>>>(a, rgb, finalT, nContrib); countLaunch(); }
+        static const int ctas = residentCtas(compositeForwardKernel<16>, RasterShape<16>::NT, 0);
+        { compositeForwardKernel<16><<<std::min(units, ctas), RasterShape<16>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
     }
 }
 

@@ -16,6 +16,7 @@
 
 #include "raster_common.cuh"
 
+#include <algorithm>
 #include <atomic>
 
 namespace u3dg {
@@ -125,22 +126,16 @@ __device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix
 }
 
 template <int PB>
-__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
-                                                                              const float *finalTIn,
-                                                                              const int *nContribIn, float *partial,
-                                                                              int useAtomics)
+__device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int by, const float *dLdRgb,
+                                              const float *finalTIn, const int *nContribIn, float *partial,
+                                              int useAtomics, float4 *sP, float4 *sQ, float4 *sR,
+                                              uint32_t (*mask)[RasterShape<PB>::NW], int &sMax, float *sWarp)
 {
     using S = RasterShape<PB>;
     constexpr int NT = S::NT, NW = S::NW;
-    __shared__ float4 sP[NT];
-    __shared__ float4 sQ[NT];
-    __shared__ float4 sR[NT];
-    __shared__ uint32_t mask[NW][NW];
-    __shared__ int sMax;
-    extern __shared__ float sWarp[]; // NW slots of NT entries x 9 sums
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const WarpBlock<PB> wb(warp, lane);
-    const int tile = tileOf<PB>(a);
+    const WarpBlock<PB> wb(warp, lane, bx, by);
+    const int tile = tileOf<PB>(a, bx, by);
     const int start = a.tileOffsets[tile], end = a.tileOffsets[tile + 1];
     const bool in0 = wb.px < a.width && wb.py0 < a.height, in1 = wb.px < a.width && wb.py1 < a.height;
     PixelState s0, s1;
@@ -172,7 +167,7 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(R
     for (int bEnd = jmax; bEnd > 0; bEnd -= NT) {
         const int bStart = max(0, bEnd - NT), cnt = bEnd - bStart;
         __syncthreads();
-        stage<PB>(rec, a.list, start + bStart + tid, tid < cnt, tid, sP, sQ, sR, mask);
+        stage<PB>(rec, a.list, start + bStart + tid, tid < cnt, tid, sP, sQ, sR, mask, bx, by);
         {
             float4 *z = reinterpret_cast<float4 *>(sWarp);
             for (int k = tid; k < NW * NT * kG2d / 4; k += NT)
@@ -233,21 +228,55 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(R
     }
 }
 
+template <int PB>
+__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
+                                                                              const float *finalTIn,
+                                                                              const int *nContribIn, float *partial,
+                                                                              int useAtomics)
+{
+    using S = RasterShape<PB>;
+    constexpr int NT = S::NT, NW = S::NW;
+    __shared__ float4 sP[NT];
+    __shared__ float4 sQ[NT];
+    __shared__ float4 sR[NT];
+    __shared__ uint32_t mask[NW][NW];
+    __shared__ int sMax, sNext;
+    extern __shared__ float sWarp[]; // NW slots of NT entries x 9 sums
+    const int units = a.blocksX * a.blocksY;
+    int *counter = a.counters + 2; // backward: counters[2..3]
+    for (int b = nextBlock(a, counter, &sNext); b < units; b = nextBlock(a, counter, &sNext))
+        backwardBlock<PB>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, useAtomics, sP, sQ,
+                          sR, mask, sMax, sWarp);
+}
+
+template <class K>
+int residentCtas(K kernel, int threads, size_t smem)
+{
+    int dev = 0, sms = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem);
+    return std::max(1, sms * std::max(1, perSm));
+}
+
 } // namespace
 
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
                              float *partial, cudaStream_t s)
 {
+    const int units = a.blocksX * a.blocksY;
+    if (units <= 0)
+        return;
     if (a.tileSize <= 8) {
-        dim3 g((a.width + 7) / 8, (a.height + 7) / 8);
         constexpr int NT = RasterShape<8>::NT, NW = RasterShape<8>::NW;
         const size_t smem = size_t(NW) * NT * kG2d * sizeof(float);
-        { compositeBackwardKernel<8><<<g, NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, 0); countLaunch(); }
+        static const int ctas = residentCtas(compositeBackwardKernel<8>, NT, smem);
+        { compositeBackwardKernel<8><<<std::min(units, ctas), NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, 0); countLaunch(); }
     } else {
-        dim3 g((a.width + 15) / 16, (a.height + 15) / 16);
         constexpr int NT = RasterShape<16>::NT, NW = RasterShape<16>::NW;
         const size_t smem = size_t(NW) * NT * kG2d * sizeof(float); // 18 KB: no opt-in needed
-        { compositeBackwardKernel<16><<<g, NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, a.tileSize > 16 ? 1 : 0); countLaunch(); }
+        static const int ctas = residentCtas(compositeBackwardKernel<16>, NT, smem);
+        { compositeBackwardKernel<16><<<std::min(units, ctas), NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, a.tileSize > 16 ? 1 : 0); countLaunch(); }
     }
 }
 

@@ -18,15 +18,15 @@ struct RasterShape {
     static constexpr int WX = PB / 8;      // warp blocks per row
 };
 
-// This thread's two pixels and its warp's 8x8 block.
+// This thread's two pixels and its warp's 8x8 block, in pixel block (bx, by).
 template <int PB>
 struct WarpBlock {
     int px, py0, py1;
     float x0, x1, y0, y1; // warp block, inclusive
-    __device__ WarpBlock(int warp, int lane)
+    __device__ WarpBlock(int warp, int lane, int bx, int by)
     {
         constexpr int WX = RasterShape<PB>::WX;
-        const int wx0 = int(blockIdx.x) * PB + (warp % WX) * 8, wy0 = int(blockIdx.y) * PB + (warp / WX) * 8;
+        const int wx0 = bx * PB + (warp % WX) * 8, wy0 = by * PB + (warp / WX) * 8;
         px = wx0 + (lane & 7);
         py0 = wy0 + (lane >> 3);
         py1 = py0 + 4;
@@ -38,23 +38,48 @@ struct WarpBlock {
 };
 
 template <int PB>
-__device__ __forceinline__ bool meets(const float4 &p, int w)
+__device__ __forceinline__ bool meets(const float4 &p, int w, int bx, int by)
 {
     constexpr int WX = RasterShape<PB>::WX;
-    const float x0 = float(int(blockIdx.x) * PB + (w % WX) * 8), y0 = float(int(blockIdx.y) * PB + (w / WX) * 8);
+    const float x0 = float(bx * PB + (w % WX) * 8), y0 = float(by * PB + (w / WX) * 8);
     return !(p.x + p.z < x0 || p.x - p.z > x0 + 7.0f || p.y + p.w < y0 || p.y - p.w > y0 + 7.0f);
 }
 
 template <int PB>
-__device__ __forceinline__ int tileOf(const RasterArgs &a)
+__device__ __forceinline__ int tileOf(const RasterArgs &a, int bx, int by)
 {
-    return (int(blockIdx.y) * PB / a.tileSize) * a.tilesX + int(blockIdx.x) * PB / a.tileSize;
+    return (by * PB / a.tileSize) * a.tilesX + bx * PB / a.tileSize;
+}
+
+// Persistent scheduling: every CTA takes pixel blocks from a device counter until none are left,
+// heaviest tile lists first (a.blockOrder), so the long lists start early and no CTA waits for a
+// second wave. Returns the next block index for the whole CTA (>= a.blocksX * a.blocksY: done); the
+// last CTA to run out resets the counter for the next launch. counter[0] hands out blocks, counter[1]
+// counts finished CTAs.
+__device__ __forceinline__ int nextBlock(const RasterArgs &a, int *counter, int *sNext)
+{
+    const int units = a.blocksX * a.blocksY;
+    __syncthreads(); // every thread is done with the previous block's shared memory
+    if (threadIdx.x == 0) {
+        int u = atomicAdd(counter, 1);
+        if (u >= units) {
+            __threadfence();
+            if (atomicAdd(counter + 1, 1) == int(gridDim.x) - 1) {
+                atomicExch(counter, 0);
+                atomicExch(counter + 1, 0);
+            }
+        }
+        *sNext = u;
+    }
+    __syncthreads();
+    const int u = *sNext;
+    return u < units ? a.blockOrder[u] : units;
 }
 
 // Stages batch entry `slot` (if valid) and the masks: mask[w][k] bit b <=> entry 32k + b meets warp w.
 template <int PB>
 __device__ __forceinline__ void stage(const float4 *rec, const int *list, int idx, bool valid, int slot, float4 *sP,
-                                      float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB>::NW])
+                                      float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB>::NW], int bx, int by)
 {
     constexpr int NW = RasterShape<PB>::NW;
     float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f);
@@ -68,7 +93,7 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
     const int warp = slot >> 5, lane = slot & 31;
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
-        const uint32_t bits = __ballot_sync(0xffffffffu, valid && meets<PB>(p, w));
+        const uint32_t bits = __ballot_sync(0xffffffffu, valid && meets<PB>(p, w, bx, by));
         if (lane == 0)
             mask[w][warp] = bits;
     }
