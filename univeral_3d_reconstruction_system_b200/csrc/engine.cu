@@ -115,6 +115,16 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     tilesX = (cam.width + st.tile_size - 1) / st.tile_size;
     tilesY = (cam.height + st.tile_size - 1) / st.tile_size;
     const size_t nn = size_t(std::max(n, 1));
+    reserveGaussians(nn);
+    if (icap == 0)
+        reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * nn));
+    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
+    launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
+}
+
+void RasterWorkspace::reserveGaussians(size_t nn)
+{
+    nn = std::max<size_t>(nn, 1);
     rec.reserve(nn);
     depthKey.reserve(nn);
     sortKeys.reserve(nn);
@@ -129,10 +139,7 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
     flags.reserve(nn);
     cov2d.reserve(nn);
-    if (icap == 0)
-        reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * nn));
-    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
-    launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
+    hist.reserve(std::max(radixHistEntries(std::max(int(nn), icap)), size_t(256)));
 }
 
 void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *desc)
@@ -321,6 +328,16 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     graphStatus.reserve(kGraphSteps);
     // Intersection buffers sized for 16 tiles per Gaussian at the capacity; they grow on demand.
     ws.reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * cap));
+    // Everything a step or a densification needs, at the capacity: no allocation during a schedule
+    // (allocations wait for the device, and pinned ones can take far longer).
+    ws.reserveGaussians(cap);
+    for (DevBuf<int> *b : {&keep, &cost, &costScan, &accCost, &accScan, &isSplit, &splitScan, &keepScan})
+        b->reserve(cap + 1);
+    firstSecond.reserve(2);
+    dScanPartial.reserve(scanPartialEntries(int(cap)) + 1);
+    hCounts.reserve(4);
+    hNormals.reserve(6 * cap);
+    normals.reserve(6 * cap);
     // The host buffers of the caller may be released after this call returns.
     U3DG_CUDA(cudaStreamSynchronize(stream));
 }

@@ -113,6 +113,7 @@ struct HostPinned {
         if (p)
             cudaFreeHost(p);
     }
+    // Grows geometrically: page-locking is slow and cudaFreeHost waits for the device.
     void reserve(size_t n)
     {
         if (n <= cap && p)
@@ -120,8 +121,9 @@ struct HostPinned {
         if (p)
             cudaFreeHost(p);
         p = nullptr;
-        U3DG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&p), std::max<size_t>(n, 1) * sizeof(T)));
-        cap = std::max<size_t>(n, 1);
+        const size_t c = std::max<size_t>(std::max(n, cap * 2), 1);
+        U3DG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&p), c * sizeof(T)));
+        cap = c;
         bumpAllocEpoch();
     }
 };
@@ -165,6 +167,8 @@ struct RasterWorkspace {
     RasterWorkspace();
     // Sizes the intersection buffers for `capacity` entries (waits for the device if they grow).
     void reserveIntersections(size_t capacity);
+    // Sizes the per-Gaussian buffers for `count` Gaussians (project() grows them on demand otherwise).
+    void reserveGaussians(size_t count);
     // Clears the overflow / abort record (stream-ordered).
     void clearCounts(cudaStream_t stream);
     // desc (may be null): the camera of a graph-captured step (see StepDesc).

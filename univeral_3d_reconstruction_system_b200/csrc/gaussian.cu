@@ -192,6 +192,8 @@ __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
 #pragma unroll
         for (int k = 0; k < kG2d; ++k)
             g[k] = 0.0f;
+        // Unrolled so the loads of several entries are in flight together; the adds stay in entry order.
+#pragma unroll 4
         for (int e = e0; e < e1; ++e) {
             const float *src = a.partial + size_t(e) * kG2d;
 #pragma unroll

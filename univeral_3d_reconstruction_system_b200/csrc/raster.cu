@@ -116,6 +116,11 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(Ra
     __shared__ uint32_t mask[NW][NW];
     __shared__ int sNext;
     const int units = a.blocksX * a.blocksY;
+    if (a.counters == nullptr) { // one CTA per pixel block (every block resident in one wave)
+        forwardBlock<PB>(a, int(blockIdx.x) % a.blocksX, int(blockIdx.x) / a.blocksX, rgb, finalT, nContrib, sP, sQ,
+                         sR, mask);
+        return;
+    }
     for (int b = nextBlock(a, a.counters, &sNext); b < units; b = nextBlock(a, a.counters, &sNext))
         forwardBlock<PB>(a, b % a.blocksX, b / a.blocksX, rgb, finalT, nContrib, sP, sQ, sR, mask);
 }
@@ -192,12 +197,18 @@ void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int 
     const int units = a.blocksX * a.blocksY;
     if (units <= 0)
         return;
-    const RasterArgs &f = a; // forward: counters[0..1]
+    // When every pixel block fits on the GPU at once, one CTA per block in natural order (no work
+    // counter); otherwise the persistent schedule on counters[0..1].
+    RasterArgs f = a;
     if (a.tileSize <= 8) {
         static const int ctas = residentCtas(compositeForwardKernel<8>, RasterShape<8>::NT, 0);
+        if (units <= ctas)
+            f.counters = nullptr;
         { compositeForwardKernel<8><<<std::min(units, ctas), RasterShape<8>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
     } else {
         static const int ctas = residentCtas(compositeForwardKernel<16>, RasterShape<16>::NT, 0);
+        if (units <= ctas)
+            f.counters = nullptr;
         { compositeForwardKernel<16><<<std::min(units, ctas), RasterShape<16>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
     }
 }
