@@ -32,8 +32,8 @@ constexpr int kThreads = 256;
 constexpr int kItemsPerThread = 4;
 constexpr int kTile = kThreads * kItemsPerThread; // items per block round
 constexpr int kWarps = kThreads / 32;
-constexpr int kRadix = 256;
 constexpr int kMaxBlocks = 148 * 8;
+constexpr int kWideBits = 11; // one pass sorts tile ids up to 2048; other sorts use 8-bit digits
 
 // Block-wide exclusive scan of one int per thread (blockDim == 256); returns the block total.
 __device__ __forceinline__ int blockExclusiveScan(int v, int &total)
@@ -78,18 +78,22 @@ __device__ __forceinline__ void chunkOf(int n, int G, int b, int &begin, int &en
     end = int(std::min<long long>(n, begin + chunk));
 }
 
+template <int DB>
 __global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int shift, int *hist,
                                                             int G)
 {
-    __shared__ int counts[kRadix];
-    counts[threadIdx.x] = 0;
+    constexpr int R = 1 << DB;
+    __shared__ int counts[R];
+    for (int d = threadIdx.x; d < R; d += kThreads)
+        counts[d] = 0;
     __syncthreads();
     int begin, end;
     chunkOf(*nPtr, G, blockIdx.x, begin, end);
     for (int i = begin + threadIdx.x; i < end; i += kThreads)
-        atomicAdd(&counts[(keys[i] >> shift) & 0xFF], 1);
+        atomicAdd(&counts[(keys[i] >> shift) & uint32_t(R - 1)], 1);
     __syncthreads();
-    hist[threadIdx.x * G + blockIdx.x] = counts[threadIdx.x];
+    for (int d = threadIdx.x; d < R; d += kThreads)
+        hist[size_t(d) * G + blockIdx.x] = counts[d];
 }
 
 // One block per digit: exclusive scan of that digit's row of G block counts; rowTotals[d] = sum.
@@ -110,26 +114,39 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G,
         rowTotals[blockIdx.x] = carry;
 }
 
+// Stable scatter of one pass with 2^DB digits. Per round of kTile items, each warp ranks its items
+// among equal digits with match-any votes and keeps per-digit counts (at most 128, one byte) in shared
+// memory; an item's position is its digit's base + the counts of the warps before it (they hold
+// earlier items) + its rank in its warp. After the round the last item of each (warp, digit) advances
+// the digit's base and clears that count, so only the touched counts are reset.
+template <int DB>
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
                                                                uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
                                                                int shift, const int *hist, const int *rowTotals, int G)
 {
-    __shared__ int warpCounts[kWarps][kRadix];
-    __shared__ int base[kRadix];
+    constexpr int R = 1 << DB;
+    __shared__ uint8_t warpCounts[kWarps][R];
+    __shared__ int base[R];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int begin, end;
     chunkOf(*nPtr, G, blockIdx.x, begin, end);
-    // Digit base: exclusive scan of the digit totals, plus this block's row prefix.
+    for (int k = threadIdx.x; k < kWarps * R; k += kThreads)
+        (&warpCounts[0][0])[k] = 0;
     {
-        int total;
-        const int ex = blockExclusiveScan(rowTotals[threadIdx.x], total);
-        base[threadIdx.x] = ex + hist[threadIdx.x * G + blockIdx.x];
+        // Digit base: exclusive scan of the digit totals, plus this block's row prefix.
+        int carry = 0;
+        for (int c0 = 0; c0 < R; c0 += kThreads) {
+            const int d = c0 + threadIdx.x;
+            int total;
+            const int ex = blockExclusiveScan(rowTotals[d], total);
+            base[d] = carry + ex + hist[size_t(d) * G + blockIdx.x];
+            carry += total;
+        }
     }
+    __syncthreads();
     const uint32_t lanesBelow = (1u << lane) - 1u;
+    uint8_t *myCounts = warpCounts[warp];
     for (int r0 = begin; r0 < end; r0 += kTile) {
-        for (int k = threadIdx.x; k < kWarps * kRadix; k += kThreads)
-            (&warpCounts[0][0])[k] = 0;
-        __syncthreads();
         const int first = r0 + warp * (32 * kItemsPerThread);
         uint32_t key[kItemsPerThread], val[kItemsPerThread];
         int digit[kItemsPerThread], local[kItemsPerThread];
@@ -139,41 +156,65 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
             const bool valid = i < end;
             key[r] = valid ? keysIn[i] : 0u;
             val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
-            const int d = valid ? int((key[r] >> shift) & 0xFF) : kRadix;
+            const int d = valid ? int((key[r] >> shift) & uint32_t(R - 1)) : R;
             digit[r] = d;
+            local[r] = 0;
             const uint32_t peers = __match_any_sync(0xffffffffu, d);
             int before = 0;
             if (valid) {
-                before = warpCounts[warp][d];
+                before = myCounts[d];
                 local[r] = before + __popc(peers & lanesBelow);
             }
             __syncwarp();
             if (valid && lane == __ffs(peers) - 1)
-                warpCounts[warp][d] = before + __popc(peers);
+                myCounts[d] = uint8_t(before + __popc(peers));
             __syncwarp();
         }
         __syncthreads();
-        // Exclusive prefix of every digit over the warps (warps hold consecutive item ranges).
-        int roundTotal = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const int c = warpCounts[w][threadIdx.x];
-            warpCounts[w][threadIdx.x] = roundTotal;
-            roundTotal += c;
-        }
-        __syncthreads();
+        bool last[kItemsPerThread];
 #pragma unroll
         for (int r = 0; r < kItemsPerThread; ++r) {
             const int d = digit[r];
-            if (d < kRadix) {
-                const int pos = base[d] + warpCounts[warp][d] + local[r];
+            last[r] = false;
+            if (d < R) {
+                int cross = 0;
+                for (int w = 0; w < warp; ++w)
+                    cross += warpCounts[w][d];
+                const int pos = base[d] + cross + local[r];
                 keysOut[pos] = key[r];
                 valsOut[pos] = val[r];
+                last[r] = local[r] == int(myCounts[d]) - 1;
             }
         }
         __syncthreads();
-        base[threadIdx.x] += roundTotal;
+#pragma unroll
+        for (int r = 0; r < kItemsPerThread; ++r)
+            if (last[r])
+                atomicAdd(&base[digit[r]], int(myCounts[digit[r]]));
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kItemsPerThread; ++r)
+            if (last[r])
+                myCounts[digit[r]] = 0;
+        __syncthreads();
     }
+}
+
+// Tile offsets of a single-pass tile sort: the exclusive scan of its digit totals (digit = tile).
+__global__ void __launch_bounds__(kThreads) digitOffsetsKernel(const int *rowTotals, int tiles, const BinCounts *c,
+                                                               int *tileOffsets)
+{
+    int carry = 0;
+    for (int c0 = 0; c0 < tiles; c0 += kThreads) {
+        const int t = c0 + threadIdx.x;
+        int total;
+        const int ex = blockExclusiveScan(t < tiles ? rowTotals[t] : 0, total);
+        if (t < tiles)
+            tileOffsets[t] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0)
+        tileOffsets[tiles] = c->effTotal;
 }
 
 // Exclusive scan, reduce-then-scan over a host-known n.
@@ -345,18 +386,30 @@ inline int grid(long long n, int t) { return int((n + t - 1) / t); }
 
 int radixBlocks(int nMax) { return std::max(1, std::min(kMaxBlocks, (nMax + kTile - 1) / kTile)); }
 
-size_t radixHistEntries(int nMax) { return size_t(kRadix) * size_t(radixBlocks(nMax)); }
+size_t radixHistEntries(int nMax) { return size_t(1 << kWideBits) * size_t(radixBlocks(nMax)); }
 
-void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
-                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s)
+int radixDigits() { return 1 << kWideBits; }
+
+int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
+                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s)
 {
     uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
     const uint32_t *vin = nullptr;
     const int G = radixBlocks(nMax);
-    for (int shift = 0; shift < bits; shift += 8) {
-        { radixHistKernel<<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
-        { radixRowScanKernel<<<kRadix, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
-        { radixScatterKernel<<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+    // Keys of up to 11 bits (tile ids) in one pass of 2048 digits; longer keys in 8-bit passes.
+    const bool wide = bits <= kWideBits;
+    const int db = wide ? kWideBits : 8;
+    int passes = 0;
+    for (int shift = 0; shift < bits; shift += db, ++passes) {
+        if (wide) {
+            { radixHistKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
+            { radixRowScanKernel<<<1 << kWideBits, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
+            { radixScatterKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+        } else {
+            { radixHistKernel<8><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
+            { radixRowScanKernel<<<1 << 8, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
+            { radixScatterKernel<8><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+        }
         uint32_t *nk = kin;
         kin = kout;
         kout = nk;
@@ -365,6 +418,7 @@ void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t 
     }
     *keysOut = kin;
     *valsOut = const_cast<uint32_t *>(vin);
+    return passes;
 }
 
 size_t scanPartialEntries(int n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
@@ -411,11 +465,14 @@ void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, in
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s)
+                        int capacity, int tiles, int *list, int *tileOffsets, const int *digitTotals, cudaStream_t s)
 {
     if (capacity > 0)
         { finalizeKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedEmit, emitGid, c, list); countLaunch(); }
-    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
+    if (digitTotals != nullptr && tiles <= (1 << kWideBits))
+        { digitOffsetsKernel<<<1, kThreads, 0, s>>>(digitTotals, tiles, c, tileOffsets); countLaunch(); }
+    else
+        { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
 }
 
 } // namespace u3dg

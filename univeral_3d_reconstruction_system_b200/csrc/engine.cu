@@ -146,7 +146,7 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
 {
     const int tiles = tilesX * tilesY;
     hist.reserve(std::max(radixHistEntries(std::max(n, icap)), size_t(256)));
-    rowTotals.reserve(256);
+    rowTotals.reserve(size_t(radixDigits()));
     tileOffsets.reserve(size_t(tiles) + 1);
     uint32_t *keysOut = nullptr, *valsOut = nullptr;
     launchSetCount(counts.p, n, stream);
@@ -161,10 +161,11 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     while ((1 << bits) < tiles)
         ++bits;
     bits = std::max(bits, 1);
-    radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits, hist.p, rowTotals.p,
+    const int tilePasses = radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits, hist.p, rowTotals.p,
                    &keysOut, &valsOut, stream);
     listEmit = valsOut;
-    launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p, stream);
+    launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p,
+                       tilePasses == 1 ? rowTotals.p : nullptr, stream);
 }
 
 void RasterWorkspace::forwardChecked(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,

@@ -89,8 +89,11 @@ size_t radixHistEntries(int nMax);
 // Stable LSD radix sort of (key, value) pairs on key bits [0, bits); the item count is read on the
 // device from *nDev (at most nMax); the initial values are the item indices. Result in *keysOut /
 // *valsOut (one of the two buffers).
-void radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
-                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s);
+// Returns the number of passes (11-bit digits); rowTotals needs radixDigits() entries and holds the
+// digit totals of the last pass.
+int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
+                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s);
+int radixDigits();
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
@@ -105,8 +108,10 @@ void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
                 int tilesX, uint32_t *keys, int *emitGid, cudaStream_t s);
 // After the tile sort: Gaussian id per sorted entry and the tile offsets.
+// digitTotals (may be null): the digit totals of a single-pass tile sort, whose exclusive scan gives the
+// tile offsets directly; otherwise they come from a binary search in the sorted keys.
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s);
+                        int capacity, int tiles, int *list, int *tileOffsets, const int *digitTotals, cudaStream_t s);
 
 // raster.cu
 struct RasterArgs {

@@ -104,8 +104,14 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
     }
 }
 
+// Resident CTAs per SM the compiler must allow for: caps registers per thread at 65536 / (NT * n)
+// (48 at 10 for NT = 128).
+#ifndef U3DG_FWD_MIN_BLOCKS
+#define U3DG_FWD_MIN_BLOCKS 10
+#endif
+
 template <int PB>
-__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
+__global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_FWD_MIN_BLOCKS) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
                                                                               int *nContrib)
 {
     using S = RasterShape<PB>;

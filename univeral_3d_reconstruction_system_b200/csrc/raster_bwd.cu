@@ -228,8 +228,19 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     }
 }
 
+// Resident CTAs per SM the compiler must allow for: caps registers per thread at 65536 / (NT * n)
+// (80 at 6 for NT = 128; without a cap ptxas takes 105 and only 4 CTAs fit).
+#ifndef U3DG_BWD_MIN_BLOCKS
+#define U3DG_BWD_MIN_BLOCKS 6
+#endif
+// Shared-memory carveout hint in percent of the maximum (negative: the driver's default). More shared
+// memory admits more CTAs but leaves less L1 for the record gathers.
+#ifndef U3DG_BWD_CARVEOUT
+#define U3DG_BWD_CARVEOUT -1
+#endif
+
 template <int PB>
-__global__ void __launch_bounds__(RasterShape<PB>::NT) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
+__global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
                                                                               const float *finalTIn,
                                                                               const int *nContribIn, float *partial,
                                                                               int useAtomics)
@@ -253,6 +264,8 @@ template <class K>
 int residentCtas(K kernel, int threads, size_t smem)
 {
     int dev = 0, sms = 0, perSm = 0;
+    if (U3DG_BWD_CARVEOUT >= 0)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, U3DG_BWD_CARVEOUT);
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem);
