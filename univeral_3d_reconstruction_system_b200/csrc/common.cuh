@@ -46,7 +46,11 @@ struct __align__(16) SplatRec {
     float A, B, C; // conic = inverse 2D covariance
     float alpha;   // sigmoid(opacity)
     float r, g, b; // clamped DC colour
-    float depth;   // camera-space depth
+    // Lowest Gaussian exponent whose alpha can reach the minimum alpha: ln(minAlpha / alpha) - 1e-4
+    // (-inf when minAlpha <= 0). Below it, alpha * expf(power) < minAlpha whatever expf's rounding
+    // (at most a few ulps, far inside the 1e-4 margin), so the compositing kernels skip the exponential
+    // for those pixels and still decide exactly as the reference does.
+    float powMin;
 };
 
 // Per-step scalars the device computes and the host reads lazily.

@@ -107,7 +107,6 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
     SplatRec r;
     r.mx = u;
     r.my = v;
-    r.depth = p.pc[2];
     r.A = p.c * invDet;
     r.B = -p.b * invDet;
     r.C = p.a * invDet;
@@ -138,6 +137,7 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
     r.g = col3[1];
     r.b = col3[2];
     r.alpha = sigmoidCR(P.opac[i]);
+    r.powMin = st.min_alpha > 0.0f ? logf(st.min_alpha / r.alpha) - 1e-4f : -__int_as_float(0x7f800000);
     // Contributing box: alpha = min(0.99, a exp(-q/2)) >= minAlpha  <=>  q <= t = 2 ln(a / minAlpha), and
     // {q <= t} lies within |dx| <= sqrt(t Sxx), |dy| <= sqrt(t Syy). The float evaluation of q in the
     // compositing kernels may differ from the exact q by a few ulps times the covariance condition

@@ -25,7 +25,7 @@ __device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const fl
 {
     const float dy = P.y - fy;
     const float power = powerAt(Q, dx, dy);
-    if (power > 0.0f)
+    if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
         return;
     const float raw = Q.w * rasterExp(power);
     const float al = (raw < kMaxAlpha) ? raw : kMaxAlpha;

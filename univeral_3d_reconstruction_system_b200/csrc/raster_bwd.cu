@@ -35,7 +35,7 @@ __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const
 {
     const float dy = __fsub_rn(P.y, s.fy);
     const float power = powerAt(Q, dx, dy);
-    if (power > 0.0f)
+    if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
         return false;
     const float G = rasterExp(power);
     const float raw = __fmul_rn(Q.w, G);

@@ -86,9 +86,12 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
     if (valid) {
         const float4 *r = rec + size_t(list[idx]) * 3;
         p = r[0];
-        sP[slot] = p;
+        const float4 c = r[2];
+        // The blending loops read the mean from sP and the exponent floor (SplatRec::powMin) from its
+        // third slot; the contributing box is only needed for the masks below.
+        sP[slot] = make_float4(p.x, p.y, c.w, p.w);
         sQ[slot] = r[1];
-        sR[slot] = r[2];
+        sR[slot] = c;
     }
     const int warp = slot >> 5, lane = slot & 31;
 #pragma unroll
