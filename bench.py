@@ -196,6 +196,23 @@ def algorithmic_bytes(n: int, v: int, i: int, p: int) -> dict:
     }
 
 
+def profiled_traffic(kernel: str) -> float | None:
+    """DRAM bytes (read + write) of one launch of `kernel` on this workload, from the committed ncu
+    summary profiles/<kernel>_high-300k.md (one `ncu --set full` capture); None without it."""
+    path = ROOT / "profiles" / f"{kernel}_high-300k.md"
+    if not path.exists():
+        return None
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    total, found = 0.0, 0
+    for line in path.read_text().splitlines():
+        for metric in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            if f"`{metric}`" in line:
+                value, unit = line.split("|")[2].split()[:2]
+                total += float(value.replace(",", "")) * scale.get(unit, 1.0)
+                found += 1
+    return total if found == 2 else None
+
+
 def run_ours(args, dist: Dist) -> dict:
     from univeral_3d_reconstruction_system_b200 import _lib, api
 
@@ -277,7 +294,10 @@ def run_ours(args, dist: Dist) -> dict:
         "roofline": {
             "bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} hbm_gbs",
-            "traffic": None, "algorithmic_bytes_per_launch": bytes_[dominant],
+            "traffic": profiled_traffic({"backward": "compositeBackwardKernel", "forward": "compositeForwardKernel",
+                                         "update": "chainKernel"}.get(dominant, dominant)),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
+            "algorithmic_bytes_per_launch": bytes_[dominant],
             "step_bytes": step_bytes, "step_achieved_gbs": round(step_bytes / (per_step_ms * 1e-3) / 1e9, 1),
         },
         "e2e": {

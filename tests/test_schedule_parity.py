@@ -7,8 +7,8 @@ deterministic with more than one thread (its backward adds per-Gaussian gradient
 four runs of the Fast preset on a 16-core host ended at 29.37, 29.40, 29.46 and 29.52 dB. The GPU run
 (deterministic) ended at 29.345 dB, 0.09 dB below their mean. One reference run per test therefore
 carries about +-0.08 dB of its own scatter, and the assertion allows 0.1 dB plus that: 0.2 dB. The
-Fast preset runs by default; Balanced and High (minutes to tens of minutes on the CPU) run when
-U3DG_FULL_PARITY=1."""
+Fast preset runs by default; U3DG_PARITY_PRESETS=fast,balanced,high selects others (Balanced takes
+about ten minutes of CPU time, High about an hour)."""
 from __future__ import annotations
 
 import os
@@ -19,7 +19,7 @@ import pytest
 from univeral_3d_reconstruction_system_b200.scenes import make_scene
 from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
 
-PRESETS = ["fast"] + (["balanced", "high"] if os.environ.get("U3DG_FULL_PARITY") == "1" else [])
+PRESETS = [p for p in os.environ.get("U3DG_PARITY_PRESETS", "fast").split(",") if p]
 
 
 @pytest.mark.gpu

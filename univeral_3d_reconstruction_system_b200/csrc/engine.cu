@@ -139,6 +139,7 @@ void RasterWorkspace::reserveGaussians(size_t nn)
     scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
     flags.reserve(nn);
     cov2d.reserve(nn);
+    g2d.reserve(nn * kG2d);
     hist.reserve(std::max(radixHistEntries(std::max(int(nn), icap)), size_t(256)));
 }
 
@@ -238,7 +239,9 @@ ChainArgs RasterWorkspace::chainArgs(const Params &P) const
     a.flags = flags.p;
     a.rankOf = rankOf.p;
     a.offs = offs.p;
+    a.sortedIds = sortedIds;
     a.partial = partial.p;
+    a.g2d = g2d.p;
     a.counts = counts.p;
     return a;
 }

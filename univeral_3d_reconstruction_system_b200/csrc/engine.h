@@ -145,6 +145,7 @@ struct RasterWorkspace {
     DevBuf<int> radius, rankOf, cnt, offs, scanPartial, hist, rowTotals;
     DevBuf<uint8_t> flags;
     DevBuf<float4> cov2d;
+    DevBuf<float> g2d; // per Gaussian: summed 2D gradients (chain-rule input)
     // per intersection (capacity icap)
     DevBuf<uint32_t> iKeys0, iKeys1, iVals0, iVals1;
     DevBuf<int> emitGid, list;

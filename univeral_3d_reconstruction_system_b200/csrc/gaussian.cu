@@ -173,12 +173,87 @@ __device__ __forceinline__ void adamOne(float &p, float &m, float &v, float g, f
     p -= stepSize * m / (sqrtf(v) * invSqrtBc2 + 1e-15f);
 }
 
+// The 9 summed 2D gradients of every Gaussian from the per-(tile, Gaussian) partials of the
+// compositing backward. Emission order is depth-rank order, so a rank's partials are contiguous: one
+// warp per 32 consecutive ranks walks their partials 32 entries at a time (coalesced), lane j holding
+// entry j of the chunk; a segmented inclusive scan over the lanes (segments = ranks) adds the entries
+// of each rank in lane order, and each rank's lane adds the scan value at its last entry in the chunk.
+// The order of the additions is fixed, so the sums are deterministic. Written per Gaussian id.
+__global__ void __launch_bounds__(256) partialSumKernel(const float *partial, const int *offs,
+                                                        const uint32_t *sortedIds, int n, const BinCounts *counts,
+                                                        float *g2d)
+{
+    if (counts != nullptr && counts->abortIter >= 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int warps = int((gridDim.x * blockDim.x) >> 5);
+    for (int w = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w * 32 < n; w += warps) {
+        const int r = w * 32 + lane;
+        const bool valid = r < n;
+        const int o = valid ? offs[r] : INT_MAX;
+        const int oEnd = valid ? offs[r + 1] : INT_MAX;
+        const int first = offs[w * 32], last = offs[min(w * 32 + 32, n)];
+        float acc[kG2d];
+#pragma unroll
+        for (int k = 0; k < kG2d; ++k)
+            acc[k] = 0.0f;
+        for (int c0 = first; c0 < last; c0 += 32) {
+            const int e = c0 + lane;
+            const bool in = e < last;
+            // Owner of entry e: the last lane whose start offset is not above e.
+            int owner = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int oc = __shfl_sync(0xffffffffu, o, owner + step);
+                if (oc <= e)
+                    owner += step;
+            }
+            float v[kG2d];
+#pragma unroll
+            for (int k = 0; k < kG2d; ++k)
+                v[k] = in ? partial[size_t(e) * kG2d + k] : 0.0f;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int ownerUp = __shfl_up_sync(0xffffffffu, owner, d);
+                const bool same = lane >= d && ownerUp == owner;
+#pragma unroll
+                for (int k = 0; k < kG2d; ++k) {
+                    const float up = __shfl_up_sync(0xffffffffu, v[k], d);
+                    if (same)
+                        v[k] = __fadd_rn(v[k], up);
+                }
+            }
+            // This lane's rank: its last entry inside the chunk, if any.
+            const int lastE = min(min(oEnd, last), c0 + 32) - 1;
+            const bool has = valid && o < c0 + 32 && oEnd > c0 && lastE >= max(o, c0);
+            const int src = has ? lastE - c0 : lane;
+#pragma unroll
+            for (int k = 0; k < kG2d; ++k) {
+                const float got = __shfl_sync(0xffffffffu, v[k], src);
+                if (has)
+                    acc[k] = __fadd_rn(acc[k], got);
+            }
+        }
+        if (valid) {
+            float *dst = g2d + size_t(sortedIds[r]) * kG2d;
+#pragma unroll
+            for (int k = 0; k < kG2d; ++k)
+                dst[k] = acc[k];
+        }
+    }
+}
+
 // Rasterizer::backward pass 2 (Rasterizer.cpp:432-544) for one Gaussian per thread, fused either with
 // Adam::step (kAdam: the trainer; gradients never leave registers) or with adding the gradients into
-// caller arrays (the unit entry point). The per-Gaussian 2D gradient is summed here from the per
-// (tile, Gaussian) partials of the compositing backward, in tile order (deterministic).
+// caller arrays (the unit entry point). The per-Gaussian 2D gradient comes from partialSumKernel.
+// Resident CTAs per SM the compiler must allow for: caps registers per thread at 65536 / (256 * n)
+// (64 at 4; the kernel is latency-bound, and 4 CTAs per SM beat fewer with more registers).
+#ifndef U3DG_CHAIN_MIN_BLOCKS
+#define U3DG_CHAIN_MIN_BLOCKS 4
+#endif
+
 template <bool kAdam>
-__global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
+__global__ void __launch_bounds__(256, U3DG_CHAIN_MIN_BLOCKS) chainKernel(ChainArgs a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n || (a.counts != nullptr && a.counts->abortIter >= 0))
@@ -186,20 +261,10 @@ __global__ void __launch_bounds__(256) chainKernel(ChainArgs a)
     const Params &P = a.params;
     float gMeans[3] = {0, 0, 0}, gScales[3] = {0, 0, 0}, gQuats[4] = {0, 0, 0, 0}, gOpac = 0, gColors[3] = {0, 0, 0};
     if (a.radius[i] > 0) {
-        const int rk = a.rankOf[i];
-        const int e0 = a.offs[rk], e1 = a.offs[rk + 1];
         float g[kG2d];
 #pragma unroll
         for (int k = 0; k < kG2d; ++k)
-            g[k] = 0.0f;
-        // Unrolled so the loads of several entries are in flight together; the adds stay in entry order.
-#pragma unroll 4
-        for (int e = e0; e < e1; ++e) {
-            const float *src = a.partial + size_t(e) * kG2d;
-#pragma unroll
-            for (int k = 0; k < kG2d; ++k)
-                g[k] += src[k];
-        }
+            g[k] = a.g2d[size_t(i) * kG2d + k];
         const u3dg_camera &cam = a.desc ? a.desc->cam : a.cam;
         const float dmx = g[0], dmy = g[1], dA = g[2], dB = g[3], dC = g[4];
         if (a.gradAccum != nullptr) {
@@ -525,6 +590,8 @@ void launchChain(const ChainArgs &a, bool adam, cudaStream_t s)
 {
     if (a.n <= 0)
         return;
+    { partialSumKernel<<<std::min(blocks((long long)(a.n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(
+          a.partial, a.offs, a.sortedIds, a.n, a.counts, a.g2d); countLaunch(); }
     if (adam)
         { chainKernel<true><<<blocks(a.n, 256), 256, 0, s>>>(a); countLaunch(); }
     else

@@ -50,7 +50,9 @@ struct ChainArgs {
     const uint8_t *flags;
     const int *rankOf;    // depth rank of every Gaussian
     const int *offs;      // per rank: first intersection in emission order (n + 1 entries)
+    const uint32_t *sortedIds; // Gaussian id per depth rank
     const float *partial; // per intersection, in emission order: 9 summed 2D gradients
+    float *g2d;           // per Gaussian: the 9 partials summed (written by launchChain's first kernel)
     const BinCounts *counts; // the kernel does nothing when counts->abortIter >= 0
     float *gradAccum;     // |dL/dmean2d| NDC statistic (may be null)
     int *gradCount;       // visibility count (may be null)
