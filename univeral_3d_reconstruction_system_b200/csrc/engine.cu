@@ -610,7 +610,12 @@ bool TrainerImpl::beginGraphChunk()
     const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
                        stepGraph.icap != ws.icap || stepGraph.epoch != allocEpoch();
     if (stale) {
-        stepGraph.reset();
+        // Keep the instantiated graph: a re-capture with the same topology (only kernel arguments and
+        // grid sizes change after a densification) updates it in place, cheaper than instantiating.
+        if (stepGraph.graph) {
+            cudaGraphDestroy(stepGraph.graph);
+            stepGraph.graph = nullptr;
+        }
         const unsigned long long epoch0 = allocEpoch();
         const unsigned long long launches0 = launchCount();
         U3DG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
@@ -637,7 +642,20 @@ bool TrainerImpl::beginGraphChunk()
             pendingSnaps.clear();
             return false;
         }
-        U3DG_CUDA(cudaGraphInstantiate(&stepGraph.exec, stepGraph.graph, 0));
+        bool updated = false;
+        if (stepGraph.exec) {
+            cudaGraphExecUpdateResultInfo info{};
+            updated = cudaGraphExecUpdate(stepGraph.exec, stepGraph.graph, &info) == cudaSuccess &&
+                      info.result == cudaGraphExecUpdateSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(stepGraph.exec);
+                stepGraph.exec = nullptr;
+            }
+        }
+        if (!updated)
+            U3DG_CUDA(cudaGraphInstantiate(&stepGraph.exec, stepGraph.graph, 0));
+        ++stepGraph.captures;
         stepGraph.n = n;
         stepGraph.cur = cur;
         stepGraph.icap = ws.icap;

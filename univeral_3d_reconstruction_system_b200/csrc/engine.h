@@ -243,7 +243,8 @@ struct StepGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long epoch = 0;
-    long long kernels = 0; // kernel nodes per launch
+    long long kernels = 0;  // kernel nodes per launch
+    long long captures = 0; // captures so far (instantiated, or applied to the instance as an update)
     int n = -1, cur = -1, icap = -1;
     void reset()
     {

@@ -244,8 +244,14 @@ def load_network(path: Path = WEIGHTS_PATH) -> api.WarmStartNet:
 # ------------------------------------------------------------------ evaluation
 
 
-def run_from(sc: Scene, init: GaussianModel, init_seconds: float, chunk: int):
+def run_from(sc: Scene, init: GaussianModel, init_seconds: float, chunk: int, iterations: int | None = None):
+    """A full schedule from `init`: the scene's preset schedule, or forIterations(iterations) with the
+    preset's Gaussian cap."""
     opt = sc.options()
+    if iterations:
+        short = TrainOptions.for_iterations(iterations)
+        short.max_gaussians = opt.max_gaussians
+        opt = short
     t = api.Trainer(init, sc.images, sc.extent, opt)
     r = run_schedule(t, opt.iterations, chunk=chunk)
     out = r.as_dict()
@@ -255,7 +261,11 @@ def run_from(sc: Scene, init: GaussianModel, init_seconds: float, chunk: int):
     return r, out
 
 
-def evaluate_seed(net: api.WarmStartNet, seed: int, chunk: int = 250, spec=None) -> dict:
+def evaluate_seed(net: api.WarmStartNet, seed: int, chunk: int = 250, spec=None,
+                  short_iterations: int | None = None) -> dict:
+    """Plain vs warm start on one held-out seed. With short_iterations, both inits also run the shorter
+    schedule forIterations(short_iterations) (the plain one as the control): whether and when each
+    reaches the plain full-schedule PSNR."""
     sc = build_scene(seed, spec if spec is not None else scene_spec(seed))
     t0 = time.perf_counter()
     plain = api.initGaussiansFromPoints(sc.init_xyz, sc.init_rgb)
@@ -269,17 +279,35 @@ def evaluate_seed(net: api.WarmStartNet, seed: int, chunk: int = 250, spec=None)
     plain_time = t_plain_init + rp.total_seconds
     ttp = rw.time_to_psnr(target)
     warm_time = None if ttp is None else t_warm_init + ttp
-    return {"seed": seed, "gt_count": sc.spec.gt_count, "target_psnr": round(target, 4),
-            "plain_time_s": round(plain_time, 4), "warm_time_to_target_s": None if warm_time is None else
-            round(warm_time, 4), "time_ratio": None if warm_time is None else round(warm_time / plain_time, 4),
-            "plain_final_psnr": round(rp.final_psnr, 4), "warm_final_psnr": round(rw.final_psnr, 4),
-            "plain_initial_psnr": round(rp.initial_psnr, 4), "warm_initial_psnr": round(rw.initial_psnr, 4),
-            "plain": dp, "warm": dw}
+    row = {"seed": seed, "gt_count": sc.spec.gt_count, "target_psnr": round(target, 4),
+           "plain_time_s": round(plain_time, 4), "warm_time_to_target_s": None if warm_time is None else
+           round(warm_time, 4), "time_ratio": None if warm_time is None else round(warm_time / plain_time, 4),
+           "plain_final_psnr": round(rp.final_psnr, 4), "warm_final_psnr": round(rw.final_psnr, 4),
+           "plain_initial_psnr": round(rp.initial_psnr, 4), "warm_initial_psnr": round(rw.initial_psnr, 4),
+           "plain": dp, "warm": dw}
+    if short_iterations:
+        for name, init, t_init in (("plain_short", plain, t_plain_init), ("warm_short", warm, t_warm_init)):
+            r, d = run_from(sc, init, t_init, chunk, short_iterations)
+            ttp = r.time_to_psnr(target)
+            row[name] = {"iterations": short_iterations, "final_psnr": round(r.final_psnr, 4),
+                         "time_to_target_s": None if ttp is None else round(t_init + ttp, 4),
+                         "time_ratio": None if ttp is None else round((t_init + ttp) / plain_time, 4),
+                         "trajectory": d}
+    return row
 
 
 def summarise(rows: list) -> dict:
     ratios = [r["time_ratio"] for r in rows if r["time_ratio"] is not None]
-    return {"seeds": [r["seed"] for r in rows],
+    extra = {}
+    for name in ("plain_short", "warm_short"):
+        if all(name in r for r in rows) and rows:
+            sr = [r[name]["time_ratio"] for r in rows]
+            got = [v for v in sr if v is not None]
+            extra[name] = {"iterations": rows[0][name]["iterations"], "reached": f"{len(got)}/{len(rows)}",
+                           "median_time_ratio": float(np.median(got)) if len(got) == len(rows) else None,
+                           "mean_final_psnr_minus_target_db": float(np.mean(
+                               [r[name]["final_psnr"] - r["target_psnr"] for r in rows]))}
+    return extra | {"seeds": [r["seed"] for r in rows],
             "reached": f"{len(ratios)}/{len(rows)}",
             "median_time_ratio": float(np.median(ratios)) if ratios else None,
             "mean_time_ratio": float(np.mean(ratios)) if ratios else None,
@@ -304,6 +332,8 @@ def main(argv=None) -> int:
     ev.add_argument("--seeds", type=int, default=len(EVAL_SEEDS))
     ev.add_argument("--chunk", type=int, default=250)
     ev.add_argument("--out", type=Path, default=None)
+    ev.add_argument("--short-iterations", type=int, default=0,
+                    help="also run both inits on forIterations(N) (the plain one as the control)")
     a = ap.parse_args(argv)
 
     def log(*m):
@@ -347,7 +377,7 @@ def main(argv=None) -> int:
     net = load_network(a.weights)
     rows = []
     for seed in EVAL_SEEDS[:a.seeds]:
-        r = evaluate_seed(net, seed, a.chunk)
+        r = evaluate_seed(net, seed, a.chunk, short_iterations=a.short_iterations or None)
         rows.append(r)
         log(f"seed {seed}: target {r['target_psnr']:.2f} dB, plain {r['plain_time_s']:.2f} s, warm "
             f"{r['warm_time_to_target_s']} s (ratio {r['time_ratio']}), final {r['plain_final_psnr']:.2f} vs "
