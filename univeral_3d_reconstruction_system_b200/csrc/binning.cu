@@ -15,9 +15,11 @@
 // an overflow into an empty bin list plus a flag the host reads later (it then grows the buffers and
 // replays the step).
 //
-// Sorting: stable 8-bit-digit LSD passes. A pass is three kernels: per-block digit histograms, a
-// per-digit scan over the blocks, and a scatter whose in-block ranks come from warp match-any votes.
-// Every block owns one contiguous chunk of the items and walks it in rounds of kTile items.
+// Sorting: stable LSD passes, 8-bit digits for the depth keys and one 11-bit pass for tile ids (up to
+// 2048 tiles; the tile offsets are then the exclusive scan of that pass's digit totals). A pass is
+// three kernels: per-block digit histograms, a per-digit scan over the blocks, and a scatter whose
+// in-block ranks come from warp match-any votes. Every block owns one contiguous chunk of the items
+// and walks it in rounds of kTile items.
 
 #include "kernels.h"
 
@@ -32,7 +34,11 @@ constexpr int kThreads = 256;
 constexpr int kItemsPerThread = 4;
 constexpr int kTile = kThreads * kItemsPerThread; // items per block round
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxBlocks = 148 * 8;
+// Blocks of a radix pass at most (each owns a contiguous chunk of the items in rounds of kTile).
+#ifndef U3DG_RADIX_MAX_BLOCKS
+#define U3DG_RADIX_MAX_BLOCKS (148 * 6)
+#endif
+constexpr int kMaxBlocks = U3DG_RADIX_MAX_BLOCKS;
 constexpr int kWideBits = 11; // one pass sorts tile ids up to 2048; other sorts use 8-bit digits
 
 // Block-wide exclusive scan of one int per thread (blockDim == 256); returns the block total.

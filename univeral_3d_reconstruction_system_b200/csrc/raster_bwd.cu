@@ -67,13 +67,29 @@ __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const
     if (raw > kMaxAlpha)
         return true; // clamped alpha: colour gradient only
     c[8] += G * dAl;
+    // The mean and conic gradients are linear in the per-pixel moments of dPow: sum dPow dx, dPow dy,
+    // dPow dx^2, dPow dx dy, dPow dy^2 here, and combine them with the conic once per list entry
+    // (finishEntry) instead of once per pixel.
     const float dPow = Q.w * dAl * G;
-    c[0] += dPow * -(Q.x * dx + Q.y * dy);
-    c[1] += dPow * -(Q.z * dy + Q.y * dx);
-    c[2] += dPow * -0.5f * dx * dx;
-    c[3] += dPow * -dx * dy;
-    c[4] += dPow * -0.5f * dy * dy;
+    const float pdx = dPow * dx, pdy = dPow * dy;
+    c[0] += pdx;
+    c[1] += pdy;
+    c[2] += pdx * dx;
+    c[3] += pdx * dy;
+    c[4] += pdy * dy;
     return true;
+}
+
+// Turns an entry's summed moments (pairGrad) into dL/dmean2d and dL/dconic (Rasterizer.cpp:405-412):
+// dmean = -(A m_x + B m_y, C m_y + B m_x), dA = -m_xx / 2, dB = -m_xy, dC = -m_yy / 2.
+__device__ __forceinline__ void finishEntry(const float4 &Q, float g[kG2d])
+{
+    const float mx = g[0], my = g[1];
+    g[0] = -(Q.x * mx + Q.y * my);
+    g[1] = -(Q.z * my + Q.y * mx);
+    g[2] = -0.5f * g[2];
+    g[3] = -g[3];
+    g[4] = -0.5f * g[4];
 }
 
 // Sum of c[0..8] over the warp: values 0..7 by reduce-scatter (xor 16/8/4 exchanges halve the
@@ -214,6 +230,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
 #pragma unroll
                 for (int q = 0; q < kG2d; ++q)
                     sum[q] += sWarp[(size_t(w) * NT + tid) * kG2d + q];
+            finishEntry(sQ[tid], sum);
             float *dst = partial + size_t(a.listEmit[start + bStart + tid]) * kG2d;
             if (useAtomics) {
 #pragma unroll
