@@ -19,12 +19,12 @@ namespace u3dg {
 namespace {
 
 // One front-to-back blending step of Rasterizer.cpp:305-318 for one pixel.
-__device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const float4 *sR, int j, float dx, float fy,
-                                      float minA, float minT, int lastIdx, float &T, float &cr, float &cg, float &cb,
-                                      int &last, bool &done)
+__device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const float4 *sR, int j, const ColumnTerms &ct,
+                                      float fy, float minA, float minT, int lastIdx, float &T, float &cr, float &cg,
+                                      float &cb, int &last, bool &done)
 {
     const float dy = P.y - fy;
-    const float power = powerAt(Q, dx, dy);
+    const float power = powerAt(Q, ct, dy);
     if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
         return;
     const float raw = Q.w * rasterExp(power);
@@ -75,12 +75,12 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
                 const int j = 32 * k + __ffs(bits) - 1;
                 bits &= bits - 1;
                 const float4 P = sP[j], Q = sQ[j];
-                const float dx = P.x - fx;
+                const ColumnTerms ct = columnTerms(Q, P.x - fx);
                 const int idx = b0 - start + j + 1;
                 if (!done0)
-                    blend(P, Q, sR, j, dx, fy0, minA, minT, idx, T0, r0, g0, b0c, last0, done0);
+                    blend(P, Q, sR, j, ct, fy0, minA, minT, idx, T0, r0, g0, b0c, last0, done0);
                 if (!done1)
-                    blend(P, Q, sR, j, dx, fy1, minA, minT, idx, T1, r1, g1, b1c, last1, done1);
+                    blend(P, Q, sR, j, ct, fy1, minA, minT, idx, T1, r1, g1, b1c, last1, done1);
                 if (done0 && done1)
                     break;
             }

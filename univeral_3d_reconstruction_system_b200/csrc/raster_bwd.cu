@@ -31,10 +31,10 @@ struct PixelState {
 
 // One back-to-front step of Rasterizer.cpp:385-416 for one pixel; adds its 9 contributions to c.
 __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const float4 *sR, int jj, float dx,
-                                         float minA, PixelState &s, float c[kG2d])
+                                         const ColumnTerms &ct, float minA, PixelState &s, float c[kG2d])
 {
     const float dy = __fsub_rn(P.y, s.fy);
-    const float power = powerAt(Q, dx, dy);
+    const float power = powerAt(Q, ct, dy);
     if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
         return false;
     const float G = rasterExp(power);
@@ -205,10 +205,11 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                 if (j < s0.nC || j < s1.nC) {
                     const float4 P = sP[jj], Q = sQ[jj];
                     const float dx = __fsub_rn(P.x, fx);
+                    const ColumnTerms ct = columnTerms(Q, dx);
                     if (j < s0.nC)
-                        act |= pairGrad(P, Q, sR, jj, dx, minA, s0, c);
+                        act |= pairGrad(P, Q, sR, jj, dx, ct, minA, s0, c);
                     if (j < s1.nC)
-                        act |= pairGrad(P, Q, sR, jj, dx, minA, s1, c);
+                        act |= pairGrad(P, Q, sR, jj, dx, ct, minA, s1, c);
                 }
                 if (__any_sync(0xffffffffu, act)) {
                     float v8;

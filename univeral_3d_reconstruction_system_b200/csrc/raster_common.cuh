@@ -103,11 +103,24 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
 }
 
 // Gaussian falloff exponent at one pixel, in the reference's operation order with no fused
-// multiply-add (Rasterizer.cpp:305-306), so every kernel decides contributions identically.
-__device__ __forceinline__ float powerAt(const float4 &Q, float dx, float dy)
+// multiply-add (Rasterizer.cpp:305-306), so every kernel decides contributions identically:
+//   power = -0.5 * ((A dx) dx + (C dy) dy) - (B dx) dy.
+// A thread's two pixels share a column, so the dx terms are computed once (columnTerms) and give the
+// same roundings as computing them per pixel.
+struct ColumnTerms {
+    float axx; // (A dx) dx
+    float bx;  // B dx
+};
+
+__device__ __forceinline__ ColumnTerms columnTerms(const float4 &Q, float dx)
 {
-    const float q = __fadd_rn(__fmul_rn(__fmul_rn(Q.x, dx), dx), __fmul_rn(__fmul_rn(Q.z, dy), dy));
-    return __fsub_rn(__fmul_rn(-0.5f, q), __fmul_rn(__fmul_rn(Q.y, dx), dy));
+    return {__fmul_rn(__fmul_rn(Q.x, dx), dx), __fmul_rn(Q.y, dx)};
+}
+
+__device__ __forceinline__ float powerAt(const float4 &Q, const ColumnTerms &c, float dy)
+{
+    const float q = __fadd_rn(c.axx, __fmul_rn(__fmul_rn(Q.z, dy), dy));
+    return __fsub_rn(__fmul_rn(-0.5f, q), __fmul_rn(c.bx, dy));
 }
 
 __device__ __forceinline__ float rasterExp(float x) { return expf(x); }
