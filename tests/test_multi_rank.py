@@ -52,3 +52,47 @@ def test_single_process_needs_no_process_group():
     d = bench.Dist(1)
     assert d.pg is None and d.max(3.5) == 3.5
     assert bench.aggregate_rate(100, 1, 0.5) == 200.0
+
+
+def _label_rank(rank: int, world: int, port: int, shard_dir: str, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, str(ROOT))
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from univeral_3d_reconstruction_system_b200.warmstart import generate_labels
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        done = []
+
+        def label_fn(seed):
+            done.append(seed)
+            rows = 3 + seed % 4
+            return np.full((rows, 134), seed, np.float32), np.full((rows, 11), -seed, np.float32)
+
+        got = generate_labels(range(10, 17), label_fn, shard_dir, rank, world, dist.barrier, log=lambda *m: None)
+        q.put((rank, done, None if got is None else (got[0][:, 0].tolist(), got[1][:, 0].tolist())))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_share_the_label_scenes(tmp_path):
+    """Warm-start label generation with two ranks: each labels every other scene (no data-path
+    collective); rank 0 then holds all rows in seed order."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_label_rank, args=(r, 2, port, str(tmp_path), q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = dict((r, (done, res)) for r, done, res in (q.get(timeout=5) for _ in range(2)))
+    assert got[0][0] == [10, 12, 14, 16] and got[1][0] == [11, 13, 15]
+    assert got[1][1] is None
+    x0, t0 = got[0][1]
+    expect = [float(s) for s in range(10, 17) for _ in range(3 + s % 4)]
+    assert x0 == expect and t0 == [-v for v in expect]

@@ -26,7 +26,8 @@ PSNR every `chunk` iterations (not timed), time-to-PSNR = initialisation wall ti
 or plain init + features + network inference) + device training time until the PSNR first reaches
 the plain run's final PSNR.
 
-Usage:  python -m univeral_3d_reconstruction_system_b200.warmstart train --out DIR
+Usage:  python -m univeral_3d_reconstruction_system_b200.warmstart train --out FILE
+        (or under torchrun, one rank per GPU: the label scenes are shared over the ranks)
         python -m univeral_3d_reconstruction_system_b200.warmstart evaluate --weights FILE
 """
 from __future__ import annotations
@@ -35,6 +36,7 @@ import argparse
 import dataclasses
 import json
 import math
+import os
 import sys
 import time
 from pathlib import Path
@@ -176,6 +178,31 @@ def label_scene(sc: Scene, iterations: int = LABEL_ITERATIONS):
     trained = t.model()
     t.close()
     return X, canonical_targets(base, trained), base
+
+
+def generate_labels(seeds, label_fn, shard_dir: Path, rank: int = 0, world: int = 1, barrier=None, log=print):
+    """Label rows of all `seeds`, the scenes shared over `world` ranks (one per GPU): rank r labels seeds
+    r, r + world, ... (scenes are independent, so there is no collective on the data) and writes each to
+    shard_dir/labels_<seed>.npz; after `barrier`, rank 0 reads every shard in seed order and returns
+    (X, T); the other ranks return None. label_fn(seed) -> (X, T)."""
+    seeds = list(seeds)
+    shard_dir = Path(shard_dir)
+    shard_dir.mkdir(parents=True, exist_ok=True)
+    t0 = time.time()
+    for k, seed in enumerate(seeds[rank::world]):
+        X, T = label_fn(seed)
+        np.savez(shard_dir / f"labels_{seed}.npz", X=X, T=T)
+        log(f"rank {rank}: label scene {k + 1} (seed {seed}): {len(X)} rows, {time.time() - t0:.1f} s")
+    if barrier is not None:
+        barrier()
+    if rank != 0:
+        return None
+    Xs, Ts = [], []
+    for seed in seeds:
+        with np.load(shard_dir / f"labels_{seed}.npz") as z:
+            Xs.append(z["X"])
+            Ts.append(z["T"])
+    return np.concatenate(Xs), np.concatenate(Ts)
 
 
 # ------------------------------------------------------------------ training
@@ -327,6 +354,8 @@ def main(argv=None) -> int:
     tr.add_argument("--scenes", type=int, default=len(TRAIN_SEEDS))
     tr.add_argument("--label-iterations", type=int, default=LABEL_ITERATIONS)
     tr.add_argument("--holdout-labels", type=int, default=2, help="held-out seeds whose label loss is reported")
+    tr.add_argument("--shard-dir", type=Path, default=None,
+                    help="where the ranks leave their label shards (default: label_shards beside --out)")
     ev = sub.add_parser("evaluate", help="plain vs warm start on held-out seeds")
     ev.add_argument("--weights", type=Path, default=WEIGHTS_PATH)
     ev.add_argument("--seeds", type=int, default=len(EVAL_SEEDS))
@@ -340,17 +369,31 @@ def main(argv=None) -> int:
         print(*m, file=sys.stderr, flush=True)
 
     if a.cmd == "train":
-        Xs, Ts = [], []
         t0 = time.time()
-        for k, seed in enumerate(TRAIN_SEEDS[:a.scenes]):
-            sc = build_scene(seed)
-            X, T, _ = label_scene(sc, a.label_iterations)
-            Xs.append(X)
-            Ts.append(T)
-            log(f"label scene {k + 1}/{a.scenes} (seed {seed}, {sc.spec.gt_count} GT): {len(X)} rows, "
-                f"{time.time() - t0:.1f} s")
-        X, T = np.concatenate(Xs), np.concatenate(Ts)
-        del Xs, Ts
+        # One process per GPU under torchrun: the label scenes are shared over the ranks, rank 0 trains.
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        barrier = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            from . import _lib
+            _lib.check(_lib.load().u3dg_set_device(int(os.environ.get("LOCAL_RANK", "0"))))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
+            barrier = dist.barrier
+
+        def label_fn(seed):
+            X, T, _ = label_scene(build_scene(seed), a.label_iterations)
+            return X, T
+
+        shard_dir = a.shard_dir or (Path(a.out).resolve().parent / "label_shards")
+        got = generate_labels(TRAIN_SEEDS[:a.scenes], label_fn, shard_dir, rank, world, barrier, log)
+        if world > 1:
+            dist.destroy_process_group()
+        if got is None:
+            return 0
+        X, T = got
         t1 = time.time()
         params, losses = train_network(X, T, log=log)
         train_s = time.time() - t1
