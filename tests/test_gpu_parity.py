@@ -11,7 +11,8 @@ import pytest
 
 from helpers import fd_setup, grad_close, make_camera, orbit_camera, random_model, rel_l2
 from univeral_3d_reconstruction_system_b200.scenes import make_scene, render_targets
-from univeral_3d_reconstruction_system_b200.types import GaussianModel, RasterSettings, TrainImage, TrainOptions, logit
+from univeral_3d_reconstruction_system_b200.types import GaussianModel, RasterSettings, RenderCamera, TrainImage, \
+    TrainOptions, logit
 
 pytestmark = pytest.mark.gpu
 
@@ -219,9 +220,10 @@ def _backward_both(u3dg, oracle, model, cam, st, w):
     return g, ndc, og, ondc
 
 
-def test_backward_matches_oracle(u3dg, oracle, tiny_scene):
+@pytest.mark.parametrize("tile", [16, 8, 32])
+def test_backward_matches_oracle(u3dg, oracle, tiny_scene, tile):
     sc = tiny_scene
-    st = RasterSettings()
+    st = RasterSettings(tile_size=tile)
     rng = np.random.default_rng(11)
     for cam in _views(sc, 3):
         w = rng.uniform(-1, 1, (cam.height, cam.width, 3)).astype(np.float32)
@@ -339,6 +341,31 @@ def test_trainer_matches_oracle_trajectory(u3dg, oracle, tiny_scene):
         assert abs(gs.loss - os_.loss) < 2e-3 * max(1.0, os_.loss)
     assert g.done()
     assert abs(g.size() - o.size()) <= max(2, o.size() // 100)
+    assert abs(g.evaluatePsnr() - o.evaluate_psnr()) < 0.1
+
+
+def test_trainer_with_views_of_two_sizes(u3dg, oracle, tiny_scene):
+    """The reference takes one camera per image, so views may differ in size (graph runs then stay
+    off): half the views at another resolution, same trajectory as the oracle."""
+    sc = tiny_scene
+    st = RasterSettings()
+    images = []
+    for k, cam in enumerate(sc.cameras):
+        if k % 2:
+            cam = RenderCamera(cam.width + 24, cam.height + 16, cam.fx * 1.25, cam.fy * 1.25,
+                               0.5 * (cam.width + 23), 0.5 * (cam.height + 15), cam.R, cam.t)
+        images.append(TrainImage(cam, TrainImage.quantize(oracle.render(sc.truth, cam, st, sc.sh_rest, 3))))
+    init = oracle.init_from_points(sc.init_xyz, sc.init_rgb)
+    opt = sc.options()
+    g = u3dg.Trainer(init, images, sc.extent, opt)
+    o = oracle.trainer(init, images, sc.extent, opt, threads=8)
+    for _ in range(2):
+        g.step(80)
+        o.step(80)
+        gs, os_ = g.stats(), o.stats()
+        assert gs.iteration == os_.iteration
+        assert abs(gs.psnr - os_.psnr) < 0.1, (gs.psnr, os_.psnr)
+    assert g.graph_launches() == 0
     assert abs(g.evaluatePsnr() - o.evaluate_psnr()) < 0.1
 
 
