@@ -252,7 +252,8 @@ def test_gpu_warmstart_applies_the_network_outputs(u3dg):
     np.testing.assert_array_equal(m.means, plain.means)
     np.testing.assert_allclose(m.scales, plain.scales + y[:, 0:3], rtol=1e-6, atol=1e-6)
     np.testing.assert_allclose(m.quats, y[:, 3:7], rtol=1e-6, atol=1e-6)
-    np.testing.assert_allclose(m.opacities, y[:, 7], rtol=1e-6, atol=1e-6)
+    floor = np.float32(-2.9444389)  # logit(0.05)
+    np.testing.assert_allclose(m.opacities, np.maximum(y[:, 7], floor), rtol=1e-6, atol=1e-6)
     np.testing.assert_allclose(m.colors, plain.colors + y[:, 8:11], rtol=1e-6, atol=1e-6)
 
 

@@ -338,6 +338,9 @@ __global__ void gatherRowsKernel(const float *src, int width, const int *rows, i
     }
 }
 
+// logit(0.05).
+constexpr float kWarmOpacityFloor = -2.9444389f;
+
 // Initial model from the plain initialisation and the network's 11 outputs: log-scales and DC colour
 // as residuals over the plain values, quaternion and logit opacity directly. Non-finite outputs fall
 // back to the plain values for that Gaussian.
@@ -358,7 +361,11 @@ __global__ void combineKernel(const float *pred, int n, float *scales, float *qu
     }
     for (int k = 0; k < 4; ++k)
         quats[4 * i + k] = y[3 + k];
-    opac[i] = y[7];
+    // Opacity floored at 0.05: the labels include Gaussians that the fixed-set runs drove transparent,
+    // and an initial opacity below the pruning threshold (0.005) would remove them at the first
+    // densification, leaving holes for the later steps to fill (held-out seeds reach the target sooner
+    // with the floor).
+    opac[i] = fmaxf(y[7], kWarmOpacityFloor);
 }
 
 } // namespace
