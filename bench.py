@@ -349,6 +349,7 @@ def run_batched(args, dist: Dist) -> dict:
     tune_s = time.time() - t1
     total = sum(opt.iterations for _, _, _, opt in scenes)
     ms = b.time_steps(max(opt.iterations for _, _, _, opt in scenes))
+    combined, recorded = b.graph_launches()
     rows = []
     seq_ms = 0.0
     for k, (init, imgs, extent, opt) in enumerate(scenes):
@@ -379,6 +380,7 @@ def run_batched(args, dist: Dist) -> dict:
            "batched_it_per_s": round(total_all / (ms * 1e-3), 1), "sequential_ms": round(seq_ms, 2),
            "sequential_it_per_s": round(total_all / (seq_ms * 1e-3), 1), "speedup": round(seq_ms / ms, 3),
            "autotune_s": round(tune_s, 2), "max_psnr_diff_db": round(max(diffs), 5),
+           "rounds_as_one_graph_launch": combined, "combined_graph_recordings": recorded,
            "per_scene": rows if dist.world == 1 else f"rank 0 scenes: {rows}"}
     log(f"batched: {out['batched_it_per_s']} it/s vs sequential {out['sequential_it_per_s']} it/s, "
         f"max PSNR diff {out['max_psnr_diff_db']} dB")

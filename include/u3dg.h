@@ -278,6 +278,10 @@ int u3dg_batch_time_steps(u3dg_batch *batch, int count, float *ms);
 int u3dg_batch_size(u3dg_batch *batch, int *scenes);
 int u3dg_batch_trainer(u3dg_batch *batch, int scene, u3dg_trainer **out);
 int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_ms_per_step);
+/* Rounds in which every unfinished scene ran its next 10 steps as one CUDA graph launch holding all
+ * scenes (scenes whose buffers stayed put since the previous round), and how often that graph was
+ * recorded. Either pointer may be NULL. */
+int u3dg_batch_graph_launches(u3dg_batch *batch, long long *launches, long long *captures);
 void u3dg_batch_destroy(u3dg_batch *batch);
 
 /* ------------------------------------------------------------------ loss */

@@ -43,6 +43,9 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
     b.step(77)
     ms = b.time_steps(50)
     assert ms > 0
+    b.step(123)  # past every scene's refine_stop: rounds of all scenes as one graph launch
+    launches, captures = b.graph_launches()
+    assert launches >= 3 and 1 <= captures <= launches
     for k, scene in enumerate(scenes):
         tile, tuned = b.tile_size(k)
         assert tile in (8, 16, 32)
@@ -51,8 +54,8 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
         else:
             assert tuned > 0
         t = b.trainer(k)
-        assert t.iteration() == 127
-        flat, st = _alone(u3dg, scene, tile, 127)
+        assert t.iteration() == 250
+        flat, st = _alone(u3dg, scene, tile, 250)
         got = t.model().flat()
         if tile == 32:
             # Tiles of 32 pixels span four CTAs that add their partial gradients atomically: the same

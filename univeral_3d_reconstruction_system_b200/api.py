@@ -208,6 +208,12 @@ class Batch:
         check(load().u3dg_batch_tile_size(self._h, scene, C.byref(tile), C.byref(ms)))
         return int(tile.value), float(ms.value)
 
+    def graph_launches(self):
+        """(rounds run as one graph launch holding every scene, recordings of that graph)."""
+        launches, captures = C.c_longlong(), C.c_longlong()
+        check(load().u3dg_batch_graph_launches(self._h, C.byref(launches), C.byref(captures)))
+        return int(launches.value), int(captures.value)
+
     def trainer(self, scene: int) -> "Trainer":
         """The scene's trainer (borrowed: valid while this batch is alive)."""
         h = C.c_void_p()

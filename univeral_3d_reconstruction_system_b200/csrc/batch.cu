@@ -15,6 +15,7 @@ struct u3dg_batch {
     std::vector<std::unique_ptr<u3dg_trainer>> scenes;
     std::vector<int> tiles;
     std::vector<float> tunedMs;
+    BatchGraph graph; // rounds of all scenes as one graph launch
     std::vector<TrainerImpl *> impls() const
     {
         std::vector<TrainerImpl *> v;
@@ -86,7 +87,7 @@ int u3dg_batch_step(u3dg_batch *batch, int count)
     return guardedCall([&] {
         u3dg_batch &b = batchOf(batch);
         if (count > 0)
-            stepBatch(b.impls(), count);
+            stepBatch(b.impls(), count, &b.graph);
     });
 }
 
@@ -112,7 +113,7 @@ int u3dg_batch_time_steps(u3dg_batch *batch, int count, float *ms)
         for (TrainerImpl *t : ts)
             U3DG_CUDA(cudaStreamWaitEvent(t->stream, start, 0));
         if (count > 0)
-            stepBatch(ts, count);
+            stepBatch(ts, count, &b.graph);
         for (size_t i = 0; i < ts.size(); ++i) {
             U3DG_CUDA(cudaEventRecord(ends[i], ts[i]->stream));
             U3DG_CUDA(cudaStreamWaitEvent(s0, ends[i], 0));
@@ -157,6 +158,17 @@ int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_m
             *tile = b.tiles[size_t(scene)];
         if (tuned_ms_per_step)
             *tuned_ms_per_step = b.tunedMs[size_t(scene)];
+    });
+}
+
+int u3dg_batch_graph_launches(u3dg_batch *batch, long long *launches, long long *captures)
+{
+    return guardedCall([&] {
+        u3dg_batch &b = batchOf(batch);
+        if (launches)
+            *launches = b.graph.launches;
+        if (captures)
+            *captures = b.graph.captures;
     });
 }
 

@@ -596,17 +596,58 @@ bool TrainerImpl::runGraphChunk()
     return endGraphChunk();
 }
 
-bool TrainerImpl::beginGraphChunk()
+void TrainerImpl::prepareGraphChunk(StepValues *vals)
 {
     constexpr int K = kGraphSteps;
     pendingSnaps.assign(K, HostSnapshot{});
-    StepValues vals[K];
     for (int k = 0; k < K; ++k) {
         pendingSnaps[k] = snapshot();
         vals[k] = nextStep();
         descHost.p[k] = vals[k].d;
         ++iteration;
     }
+}
+
+void TrainerImpl::recordGraphChunk(const StepValues *vals)
+{
+    for (int k = 0; k < kGraphSteps; ++k)
+        launchStep(vals[k], descDev.p + k, graphStatus.p + k);
+    U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
+}
+
+void TrainerImpl::uploadGraphChunk(cudaStream_t s)
+{
+    U3DG_CUDA(cudaMemcpyAsync(descDev.p, descHost.p, kGraphSteps * sizeof(StepDesc), cudaMemcpyHostToDevice, s));
+}
+
+void TrainerImpl::abandonGraphChunk()
+{
+    restore(pendingSnaps[0]);
+    pendingSnaps.clear();
+}
+
+// Makes `exec` run `graph`: an in-place update when the topology allows it, else a new instance.
+static void applyGraph(cudaGraphExec_t &exec, cudaGraph_t graph)
+{
+    bool updated = false;
+    if (exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        updated = cudaGraphExecUpdate(exec, graph, &info) == cudaSuccess && info.result == cudaGraphExecUpdateSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+    }
+    if (!updated)
+        U3DG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+}
+
+bool TrainerImpl::beginGraphChunk()
+{
+    constexpr int K = kGraphSteps;
+    StepValues vals[K];
+    prepareGraphChunk(vals);
     const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
                        stepGraph.icap != ws.icap || stepGraph.epoch != allocEpoch();
     if (stale) {
@@ -620,9 +661,7 @@ bool TrainerImpl::beginGraphChunk()
         const unsigned long long launches0 = launchCount();
         U3DG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
         try {
-            for (int k = 0; k < K; ++k)
-                launchStep(vals[k], descDev.p + k, graphStatus.p + k);
-            U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
+            recordGraphChunk(vals);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(stream, &g);
@@ -638,30 +677,17 @@ bool TrainerImpl::beginGraphChunk()
         if (allocEpoch() != epoch0) {
             // A buffer moved while the steps were being recorded: the graph may hold stale addresses.
             stepGraph.reset();
-            restore(pendingSnaps[0]);
-            pendingSnaps.clear();
+            abandonGraphChunk();
             return false;
         }
-        bool updated = false;
-        if (stepGraph.exec) {
-            cudaGraphExecUpdateResultInfo info{};
-            updated = cudaGraphExecUpdate(stepGraph.exec, stepGraph.graph, &info) == cudaSuccess &&
-                      info.result == cudaGraphExecUpdateSuccess;
-            if (!updated) {
-                cudaGetLastError();
-                cudaGraphExecDestroy(stepGraph.exec);
-                stepGraph.exec = nullptr;
-            }
-        }
-        if (!updated)
-            U3DG_CUDA(cudaGraphInstantiate(&stepGraph.exec, stepGraph.graph, 0));
+        applyGraph(stepGraph.exec, stepGraph.graph);
         ++stepGraph.captures;
         stepGraph.n = n;
         stepGraph.cur = cur;
         stepGraph.icap = ws.icap;
         stepGraph.epoch = allocEpoch();
     }
-    U3DG_CUDA(cudaMemcpyAsync(descDev.p, descHost.p, K * sizeof(StepDesc), cudaMemcpyHostToDevice, stream));
+    uploadGraphChunk(stream);
     U3DG_CUDA(cudaGraphLaunch(stepGraph.exec, stream));
     addLaunches(stepGraph.kernels);
     ++graphChunks;
@@ -690,7 +716,101 @@ bool TrainerImpl::endGraphChunk()
     return true;
 }
 
-void stepBatch(const std::vector<TrainerImpl *> &trainers, int count)
+BatchGraph::~BatchGraph()
+{
+    if (exec)
+        cudaGraphExecDestroy(exec);
+    if (graph)
+        cudaGraphDestroy(graph);
+    for (cudaEvent_t e : events)
+        cudaEventDestroy(e);
+}
+
+std::vector<long long> BatchGraph::keyOf(const std::vector<TrainerImpl *> &ts)
+{
+    std::vector<long long> k;
+    for (TrainerImpl *t : ts) {
+        k.push_back(reinterpret_cast<long long>(t));
+        k.push_back(t->n);
+        k.push_back(t->cur);
+        k.push_back(t->ws.icap);
+    }
+    k.push_back((long long)allocEpoch());
+    return k;
+}
+
+// One round of kGraphSteps steps of every trainer in `ts` as ONE graph launch: the scenes' step
+// chunks are recorded on their own streams, forked from and joined into the first trainer's stream,
+// so the graph runs them concurrently. Returns false (state untouched) if the capture had to be
+// dropped because a buffer moved.
+static bool runCombinedRound(const std::vector<TrainerImpl *> &ts, BatchGraph &bg)
+{
+    constexpr int K = TrainerImpl::kGraphSteps;
+    std::vector<std::vector<StepValues>> vals(ts.size(), std::vector<StepValues>(K));
+    for (size_t i = 0; i < ts.size(); ++i)
+        ts[i]->prepareGraphChunk(vals[i].data());
+    cudaStream_t s0 = ts[0]->stream;
+    const std::vector<long long> key = BatchGraph::keyOf(ts);
+    if (bg.exec == nullptr || key != bg.key) {
+        if (bg.graph) {
+            cudaGraphDestroy(bg.graph);
+            bg.graph = nullptr;
+        }
+        while (bg.events.size() < ts.size()) {
+            cudaEvent_t e;
+            U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            bg.events.push_back(e);
+        }
+        const unsigned long long epoch0 = allocEpoch();
+        const unsigned long long launches0 = launchCount();
+        U3DG_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
+        try {
+            U3DG_CUDA(cudaEventRecord(bg.events[0], s0)); // fork
+            for (size_t i = 1; i < ts.size(); ++i)
+                U3DG_CUDA(cudaStreamWaitEvent(ts[i]->stream, bg.events[0], 0));
+            for (size_t i = 0; i < ts.size(); ++i)
+                ts[i]->recordGraphChunk(vals[i].data());
+            for (size_t i = 1; i < ts.size(); ++i) { // join
+                U3DG_CUDA(cudaEventRecord(bg.events[i], ts[i]->stream));
+                U3DG_CUDA(cudaStreamWaitEvent(s0, bg.events[i], 0));
+            }
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s0, &g);
+            if (g)
+                cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        U3DG_CUDA(cudaStreamEndCapture(s0, &bg.graph));
+        bg.kernels = (long long)(launchCount() - launches0);
+        addLaunches(-bg.kernels);
+        if (allocEpoch() != epoch0) {
+            cudaGraphDestroy(bg.graph);
+            bg.graph = nullptr;
+            bg.key.clear();
+            for (TrainerImpl *t : ts)
+                t->abandonGraphChunk();
+            return false;
+        }
+        applyGraph(bg.exec, bg.graph);
+        bg.key = key;
+        ++bg.captures;
+    }
+    for (TrainerImpl *t : ts)
+        t->uploadGraphChunk(s0);
+    U3DG_CUDA(cudaGraphLaunch(bg.exec, s0));
+    addLaunches(bg.kernels);
+    ++bg.launches;
+    U3DG_CUDA(cudaStreamSynchronize(s0));
+    for (TrainerImpl *t : ts) {
+        ++t->graphChunks;
+        t->endGraphChunk();
+    }
+    return true;
+}
+
+void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph *bg)
 {
     const size_t S = trainers.size();
     std::vector<int> target(S);
@@ -698,13 +818,41 @@ void stepBatch(const std::vector<TrainerImpl *> &trainers, int count)
         target[i] = std::min(trainers[i]->iteration + std::max(count, 0), trainers[i]->o.iterations);
     std::vector<char> launched(S);
     for (;;) {
-        bool any = false;
+        // Every unfinished scene can run a graph chunk and all are on one device: one launch for all of
+        // them, once their buffers have stayed put for a round (otherwise each densification of any
+        // scene would re-record the whole graph).
+        std::vector<TrainerImpl *> active;
+        std::vector<int> activeTarget;
+        bool allEligible = true;
+        for (size_t i = 0; i < S; ++i) {
+            TrainerImpl &t = *trainers[i];
+            if (t.iteration >= target[i] || t.cams.empty())
+                continue;
+            active.push_back(&t);
+            activeTarget.push_back(target[i]);
+            allEligible = allEligible && t.graphEligible(target[i]) && t.device == trainers[0]->device;
+        }
+        if (active.empty())
+            break;
+        if (bg != nullptr && active.size() >= 2 && allEligible) {
+            U3DG_CUDA(cudaSetDevice(active[0]->device));
+            for (TrainerImpl *t : active)
+                t->finish();
+            bool still = true;
+            for (size_t i = 0; i < active.size(); ++i)
+                still = still && active[i]->graphEligible(activeTarget[i]);
+            const std::vector<long long> key = BatchGraph::keyOf(active);
+            if (still && (key == bg->key || key == bg->lastKey)) {
+                runCombinedRound(active, *bg);
+                continue;
+            }
+            bg->lastKey = key;
+        }
         std::fill(launched.begin(), launched.end(), 0);
         for (size_t i = 0; i < S; ++i) {
             TrainerImpl &t = *trainers[i];
             if (t.iteration >= target[i] || t.cams.empty())
                 continue;
-            any = true;
             U3DG_CUDA(cudaSetDevice(t.device));
             if (t.graphEligible(target[i])) {
                 t.finish();
@@ -721,8 +869,6 @@ void stepBatch(const std::vector<TrainerImpl *> &trainers, int count)
                 U3DG_CUDA(cudaSetDevice(trainers[i]->device));
                 trainers[i]->endGraphChunk();
             }
-        if (!any)
-            break;
     }
     for (TrainerImpl *t : trainers) {
         U3DG_CUDA(cudaSetDevice(t->device));

@@ -367,6 +367,13 @@ public:
     // capture had to be discarded, with the state restored); end waits and checks the statuses.
     bool beginGraphChunk();
     bool endGraphChunk();
+    // The parts of beginGraphChunk, for a graph that holds several trainers' chunks (stepBatch):
+    // advance the host state by kGraphSteps steps, record their launches on this trainer's stream
+    // (inside a capture), upload their descriptors on stream s, or undo the host-state advance.
+    void prepareGraphChunk(StepValues *vals);
+    void recordGraphChunk(const StepValues *vals);
+    void uploadGraphChunk(cudaStream_t s);
+    void abandonGraphChunk();
 
 private:
     std::vector<HostSnapshot> pendingSnaps; // host state before each step of the chunk in flight
@@ -381,10 +388,27 @@ struct DensifyResult {
 };
 DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng);
 
+// One CUDA graph holding a round of kGraphSteps steps of several trainers (stepBatch), with what it
+// was recorded for.
+struct BatchGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> key, lastKey; // trainers, their sizes and buffers, allocation count
+    std::vector<cudaEvent_t> events;     // fork / join events of the recording
+    long long kernels = 0, captures = 0, launches = 0;
+    static std::vector<long long> keyOf(const std::vector<TrainerImpl *> &ts);
+    BatchGraph() = default;
+    BatchGraph(const BatchGraph &) = delete;
+    BatchGraph &operator=(const BatchGraph &) = delete;
+    ~BatchGraph();
+};
+
 // Steps every trainer by `count` iterations (or to its end), interleaving them on their own streams:
 // each round launches a graph chunk (or up to kGraphSteps single steps) per trainer before waiting
-// for any, so small scenes run concurrently on the GPU.
-void stepBatch(const std::vector<TrainerImpl *> &trainers, int count);
+// for any, so small scenes run concurrently on the GPU. When every unfinished trainer can run a graph
+// chunk and their buffers have not moved since the previous round, the round is ONE launch of a
+// graph holding all of their chunks (bg, may be null: no combined graph).
+void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph *bg = nullptr);
 
 // Tile size (8, 16 or 32) with the shortest step time for a scene, timed on throwaway trainers
 // started from the same model (the batch depth of the compositing kernels follows the tile size:
