@@ -1,6 +1,7 @@
 // warmstart.cu - learned warm-start: neighbourhood features, a small FP32 MLP (forward, backward, Adam)
 // and its inference into an initial GaussianModel. No reference counterpart: the reference initialises
-// with initGaussiansFromPoints (GaussianModel.cpp:68-144), which stays the fallback and the judge.
+// with initGaussiansFromPoints (GaussianModel.cpp:68-144), which stays the fallback and the reference
+// point of every comparison.
 //
 // Features (134 floats per SfM point):
 //   [0, 48)    relative positions of the 16 nearest points, divided by the point's plain-init scale

@@ -6,7 +6,7 @@ rotation, opacity logit(0.1), DC colour from the point colour. Here a small netw
 (134 -> 128 -> 128 -> 128 -> 11, FP32, ReLU; kernels in csrc/warmstart.cu) predicts, per SfM point,
 a better starting value of those attributes from the point's 16-NN neighbourhood and colour samples
 of the views that see it. The plain initialisation stays the fallback (no network, or a non-finite
-output) and the judge (every comparison runs the same scene from both).
+output) and the reference point (every comparison runs the same scene from both).
 
 Labels (what "converged" means here): for a seeded synthetic scene, the plain trainer runs from the
 plain initialisation for LABEL_ITERATIONS with densification and opacity reset switched off, so
