@@ -352,8 +352,8 @@ int u3dg_render_views_sh(const u3dg_model *model, const float *sh_rest, int degr
 
 /* No reference counterpart: the reference initialises with initGaussiansFromPoints
  * (engine/src/splat/GaussianModel.cpp:68-144), which stays the fallback and the reference point of
- * every comparison. A small FP32 MLP (134 -> 128 -> 128 -> 128 -> 11, ReLU) maps each SfM point's neighbourhood feature to its initial
- * Gaussian: residual log-scales and DC colour over the plain initialisation, quaternion and logit
+ * every comparison. A small FP32 MLP (134 -> 128 -> 128 -> 128 -> 11, ReLU) maps each SfM point's
+ * neighbourhood feature to its initial Gaussian: residual log-scales and DC colour over the plain initialisation, quaternion and logit
  * opacity. Features (134 floats per point): 16 nearest points' relative positions (divided by the
  * plain-init scale, 48) and log distances (16), their colours (48), colour samples minus 0.5 from the 7
  * nearest views that see the point (21), and the fraction of those views found (1). Training, inference
