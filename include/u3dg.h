@@ -391,7 +391,9 @@ int u3dg_knn(const float *queries, size_t nq, const float *points, size_t np, in
 int u3dg_warmstart_features(const float *xyz, const float *rgb, size_t n, const u3dg_image *images, int count,
                             float *features);
 /* Initial model of n points through the network (out: n Gaussians); mlp == NULL gives exactly
- * initGaussiansFromPoints. A point whose prediction is not finite keeps its plain initialisation. */
+ * initGaussiansFromPoints. A point whose prediction is not finite keeps its plain initialisation; the
+ * predicted opacity is floored at 0.05 (below the pruning threshold the first densification would
+ * remove the Gaussian). */
 int u3dg_warmstart_init(u3dg_mlp *mlp, const float *xyz, const float *rgb, size_t n, const u3dg_image *images,
                         int count, u3dg_model *out);
 
