@@ -167,6 +167,8 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     const int nMax = max(s0.nC, s1.nC);
     if (nMax > 0)
         atomicMax(&sMax, nMax);
+    // This warp's pixels have no contributor at or beyond wMax: the warp skips those entries.
+    const int wMax = __reduce_max_sync(0xffffffffu, nMax);
     __syncthreads();
     const int jmax = sMax;
     // Entries behind every pixel's last contributor get no gradient (the reference's per-tile
@@ -192,6 +194,11 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
         __syncthreads();
         for (int k = NW - 1; k >= 0; --k) {
             uint32_t bits = mask[warp][k];
+            const int lim = wMax - bStart - 32 * k; // entries of this group below wMax
+            if (lim <= 0)
+                continue;
+            if (lim < 32)
+                bits &= (1u << lim) - 1u;
             while (bits) {
                 const int hb = 31 - __clz(bits);
                 bits &= ~(1u << hb);
