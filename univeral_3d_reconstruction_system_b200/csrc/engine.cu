@@ -9,6 +9,12 @@
 // wait for the GPU anyway (the split count decides how many samples the host RNG draws).
 // The training RNG (std::mt19937, Trainer.h:79) stays on the host so the view order and the split
 // samples are the reference's exactly.
+//
+// Runs of 10 steps with no densification or opacity reset among them go through a CUDA graph whose
+// kernels read each step's camera, target and learning rates from device descriptors (StepDesc); the
+// graph is recorded once and updated in place when the model size or buffers change. stepBatch runs
+// several trainers this way, as one graph launch per round when all of them can. Every buffer a
+// schedule needs is allocated when the trainer is created, so a schedule never waits on an allocation.
 
 #include "engine.h"
 
