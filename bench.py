@@ -196,21 +196,25 @@ def algorithmic_bytes(n: int, v: int, i: int, p: int) -> dict:
     }
 
 
-def profiled_traffic(kernel: str) -> float | None:
-    """DRAM bytes (read + write) of one launch of `kernel` on this workload, from the committed ncu
-    summary profiles/<kernel>_high-300k.md (one `ncu --set full` capture); None without it."""
+def profiled_metric(kernel: str, metric: str) -> float | None:
+    """One metric of one launch of `kernel` on this workload, from the committed ncu summary
+    profiles/<kernel>_high-300k.md (one `ncu --set full` capture), in base units (bytes, %, ...);
+    None without it."""
     path = ROOT / "profiles" / f"{kernel}_high-300k.md"
     if not path.exists():
         return None
     scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
-    total, found = 0.0, 0
     for line in path.read_text().splitlines():
-        for metric in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
-            if f"`{metric}`" in line:
-                value, unit = line.split("|")[2].split()[:2]
-                total += float(value.replace(",", "")) * scale.get(unit, 1.0)
-                found += 1
-    return total if found == 2 else None
+        if line.startswith(f"| `{metric}`"):
+            value, *unit = line.split("|")[2].split()
+            return float(value.replace(",", "")) * scale.get(unit[0] if unit else "", 1.0)
+    return None
+
+
+def profiled_traffic(kernel: str) -> float | None:
+    """DRAM bytes (read + write) of one launch of `kernel` (profiled_metric); None without them."""
+    r, w = profiled_metric(kernel, "dram__bytes_read.sum"), profiled_metric(kernel, "dram__bytes_write.sum")
+    return None if r is None or w is None else r + w
 
 
 def run_ours(args, dist: Dist) -> dict:
@@ -283,6 +287,8 @@ def run_ours(args, dist: Dist) -> dict:
         peaks = json.loads(pk.read_text())
     peak, peak_src = (float(peaks["hbm_gbs"]), "measured") if "hbm_gbs" in peaks else (6650.0, "fallback")
     achieved = bytes_[dominant] / (phase_ms[dominant] * 1e-3) / 1e9
+    dominant_kernel = {"backward": "compositeBackwardKernel", "forward": "compositeForwardKernel",
+                       "update": "chainKernel"}.get(dominant, dominant)
     step_bytes = sum(bytes_.values())
     per_step_ms = ms / K
     res = {
@@ -294,9 +300,13 @@ def run_ours(args, dist: Dist) -> dict:
         "roofline": {
             "bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} hbm_gbs",
-            "traffic": profiled_traffic({"backward": "compositeBackwardKernel", "forward": "compositeForwardKernel",
-                                         "update": "chainKernel"}.get(dominant, dominant)),
+            "traffic": profiled_traffic(dominant_kernel),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
+            # The compositing kernels move few bytes per instruction: their limiter is instruction
+            # issue (FP32 / integer pipes), which the same capture reports.
+            "issue_active_pct": profiled_metric(dominant_kernel, "smsp__issue_active.avg.pct_of_peak_sustained_active"),
+            "dram_throughput_pct": profiled_metric(dominant_kernel,
+                                                   "gpu__dram_throughput.avg.pct_of_peak_sustained_elapsed"),
             "algorithmic_bytes_per_launch": bytes_[dominant],
             "step_bytes": step_bytes, "step_achieved_gbs": round(step_bytes / (per_step_ms * 1e-3) / 1e9, 1),
         },
@@ -325,10 +335,11 @@ def run_ours(args, dist: Dist) -> dict:
 
 def run_batched(args, dist: Dist) -> dict:
     """Batched multi-scene training: 16 seeded scenes (scenes.batched_specs) trained together by one
-    u3dg_batch (per-scene streams, step graphs, tile sizes from the autotuner), then each scene alone
-    with its tuned tile size. Reports the aggregate iterations/s of both and every scene's PSNR. With
-    N ranks, rank r takes scenes r, r + N, ... (scenes are independent: no collective on the data
-    path); the rates are total iterations over the slowest rank's time."""
+    u3dg_batch (per-scene streams, step graphs, tile sizes and compositing batch depths from the
+    autotuner), then each scene alone with its tuned tile size and batch depth. Reports the aggregate
+    iterations/s of both and every scene's PSNR. With N ranks, rank r takes scenes r, r + N, ...
+    (scenes are independent: no collective on the data path); the rates are total iterations over the
+    slowest rank's time."""
     from univeral_3d_reconstruction_system_b200 import api
     from univeral_3d_reconstruction_system_b200.scenes import batched_specs, make_scene
     from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
@@ -353,15 +364,17 @@ def run_batched(args, dist: Dist) -> dict:
     rows = []
     seq_ms = 0.0
     for k, (init, imgs, extent, opt) in enumerate(scenes):
-        tile, tuned = b.tile_size(k)
+        tile, fwd_depth, bwd_depth, tuned = b.schedule(k)
         tb = b.trainer(k)
         p_batch = tb.evaluatePsnr()
         o2 = dataclasses.replace(opt, raster=dataclasses.replace(opt.raster, tile_size=tile))
         t = api.Trainer(init, imgs, extent, o2)
+        t.set_batch_depth(fwd_depth, bwd_depth)
         seq_ms += t.time_steps(opt.iterations)
         p_alone = t.evaluatePsnr()
         rows.append({"scene": specs[k].name, "gt": specs[k].gt_count, "views": specs[k].views,
                      "width": specs[k].width, "iterations": opt.iterations, "tile": tile,
+                     "batch_depths": [fwd_depth, bwd_depth],
                      "tuned_ms_per_step": round(tuned, 4), "gaussians": tb.size(), "psnr_batched": round(p_batch, 4),
                      "psnr_alone": round(p_alone, 4)})
         t.close()

@@ -439,6 +439,14 @@ public:
         check(u3dg_batch_tile_size(m_b, scene, &t, nullptr));
         return t;
     }
+    // List entries each forward / backward compositing thread stages per batch (1 or 2), chosen with
+    // the tile size.
+    std::pair<int, int> batchDepths(int scene) const
+    {
+        int f = 0, b = 0;
+        check(u3dg_batch_schedule(m_b, scene, nullptr, &f, &b, nullptr));
+        return {f, b};
+    }
     // The scene's model, copied back from the GPU.
     GaussianModel model(int scene) const
     {

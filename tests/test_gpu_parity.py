@@ -437,6 +437,32 @@ def test_graph_steps_match_step_by_step_launches(u3dg, oracle, tiny_scene):
                                                                    runs[0][1].psnr, runs[0][1].gaussians)
 
 
+@pytest.mark.parametrize("tile", [16, 8])
+def test_batch_depth_changes_no_result(u3dg, oracle, tiny_scene, tile):
+    """Compositing with 2 list entries staged per thread per shared-memory batch (half the block
+    barriers) gives bit-identical models to 1 entry per thread, in the forward and the backward kernel,
+    for depths set before training and switched between graph runs; other depths are rejected."""
+    sc = tiny_scene
+    init = oracle.init_from_points(sc.init_xyz, sc.init_rgb)
+    opt = sc.options()
+    opt.raster.tile_size = tile
+    runs = []
+    for first, second in (((1, 1), (1, 1)), ((2, 2), (2, 2)), ((2, 1), (1, 2))):
+        t = u3dg.Trainer(init, sc.images, sc.extent, opt)
+        t.set_batch_depth(*first)
+        t.step(63)
+        t.set_batch_depth(*second)
+        t.step(80)
+        runs.append((t.model().flat(), t.stats()))
+    for flat, st in runs[1:]:
+        np.testing.assert_array_equal(flat, runs[0][0])
+        assert (st.loss, st.psnr, st.gaussians) == (runs[0][1].loss, runs[0][1].psnr, runs[0][1].gaussians)
+    t = u3dg.Trainer(init, sc.images, sc.extent, opt)
+    for bad in ((3, 1), (1, 0)):
+        with pytest.raises(u3dg.U3dgError):
+            t.set_batch_depth(*bad)
+
+
 def test_training_recovers_a_synthetic_scene(u3dg, oracle):
     """training_recovers_a_synthetic_scene (test_splat.cpp:227-268) on the GPU."""
     rng = np.random.default_rng(11)

@@ -13,8 +13,7 @@ using namespace u3dg;
 struct u3dg_batch {
     int device = 0;
     std::vector<std::unique_ptr<u3dg_trainer>> scenes;
-    std::vector<int> tiles;
-    std::vector<float> tunedMs;
+    std::vector<RasterSchedule> schedules; // tile size, batch depths, tuned ms per step (0: not tuned)
     BatchGraph graph; // rounds of all scenes as one graph launch
     std::vector<TrainerImpl *> impls() const
     {
@@ -67,15 +66,16 @@ int u3dg_batch_create(const u3dg_model *initial, const u3dg_image *const *images
                                          !initial[s].opacities || !initial[s].colors))
                 throw StatusError(U3DG_ERR_INVALID_ARG, "scene " + std::to_string(s) + ": model has NULL arrays");
             u3dg_train_options o = options[s];
-            float ms = 0.0f;
+            RasterSchedule rs{o.raster.tile_size, 1, 1, 0.0f};
             if (autotune)
-                o.raster.tile_size =
-                    autotuneTileSize(initial[s], images[s], image_counts[s], extents[s], options[s], &ms);
+                rs = autotuneSchedule(initial[s], images[s], image_counts[s], extents[s], options[s]);
+            o.raster.tile_size = rs.tileSize;
             auto t = std::make_unique<u3dg_trainer>();
             t->impl = std::make_unique<TrainerImpl>(initial[s], images[s], image_counts[s], extents[s], o);
+            t->impl->ws.forwardDepth = rs.forwardDepth;
+            t->impl->ws.backwardDepth = rs.backwardDepth;
             t->ownedByBatch = true;
-            b->tiles.push_back(o.raster.tile_size);
-            b->tunedMs.push_back(ms);
+            b->schedules.push_back(rs);
             b->scenes.push_back(std::move(t));
         }
         *out = b.release();
@@ -151,13 +151,24 @@ int u3dg_batch_trainer(u3dg_batch *batch, int scene, u3dg_trainer **out)
 
 int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_ms_per_step)
 {
+    return u3dg_batch_schedule(batch, scene, tile, nullptr, nullptr, tuned_ms_per_step);
+}
+
+int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_depth, int *backward_depth,
+                        float *tuned_ms_per_step)
+{
     return guardedCall([&] {
         u3dg_batch &b = batchOf(batch);
         requireScene(b, scene);
+        const RasterSchedule &rs = b.schedules[size_t(scene)];
         if (tile)
-            *tile = b.tiles[size_t(scene)];
+            *tile = rs.tileSize;
+        if (forward_depth)
+            *forward_depth = rs.forwardDepth;
+        if (backward_depth)
+            *backward_depth = rs.backwardDepth;
         if (tuned_ms_per_step)
-            *tuned_ms_per_step = b.tunedMs[size_t(scene)];
+            *tuned_ms_per_step = rs.msPerStep;
     });
 }
 

@@ -210,6 +210,8 @@ RasterArgs RasterWorkspace::rasterArgs() const
     a.blocksY = (cam.height + pb - 1) / pb;
     a.blockOrder = blockOrder.p;
     a.counters = blockCounters.p;
+    a.forwardDepth = forwardDepth;
+    a.backwardDepth = backwardDepth;
     return a;
 }
 
@@ -882,42 +884,53 @@ void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph
     }
 }
 
-int autotuneTileSize(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
-                     const u3dg_train_options &opt, float *msPerStep)
+RasterSchedule autotuneSchedule(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
+                                const u3dg_train_options &opt)
 {
     static const int kTiles[3] = {16, 8, 32};
-    int best = opt.raster.tile_size;
-    float bestMs = 0.0f;
+    RasterSchedule best{opt.raster.tile_size, 1, 1, 0.0f};
     for (int tile : kTiles) {
-        u3dg_train_options o = opt;
-        o.raster.tile_size = tile;
-        o.iterations = std::max(o.iterations, 64);
-        TrainerImpl t(initial, imgs, count, extent, o);
-        t.stepTo(3 + TrainerImpl::kGraphSteps); // warm-up, including the first graph capture
-        t.finish();
-        cudaEvent_t a, b;
-        U3DG_CUDA(cudaEventCreate(&a));
-        U3DG_CUDA(cudaEventCreate(&b));
-        U3DG_CUDA(cudaEventRecord(a, t.stream));
-        t.stepTo(t.iteration + 2 * TrainerImpl::kGraphSteps);
-        t.finish();
-        U3DG_CUDA(cudaEventRecord(b, t.stream));
-        U3DG_CUDA(cudaEventSynchronize(b));
-        float ms = 0.0f;
-        U3DG_CUDA(cudaEventElapsedTime(&ms, a, b));
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-        ms /= float(2 * TrainerImpl::kGraphSteps);
-        // Tile 32 spans four CTAs per tile that add partial gradients atomically (run-to-run float
-        // differences); it has to be clearly faster than the deterministic sizes to be chosen.
-        const float need = tile > 16 ? 0.97f : 1.0f;
-        if (bestMs == 0.0f || ms < need * bestMs) {
-            bestMs = ms;
-            best = tile;
+        // Per depth: the step time of graph runs, then the compositing kernels' share from profiled
+        // steps. The forward and backward depths are picked independently (the kernels do not interact),
+        // and the tile's step time is that of depth 1 corrected by the gains of the picked depths.
+        float stepMs[2] = {}, fwdMs[2] = {}, bwdMs[2] = {};
+        for (int d = 0; d < 2; ++d) {
+            u3dg_train_options o = opt;
+            o.raster.tile_size = tile;
+            o.iterations = std::max(o.iterations, 64);
+            TrainerImpl t(initial, imgs, count, extent, o);
+            t.ws.forwardDepth = t.ws.backwardDepth = d + 1;
+            t.stepTo(3 + TrainerImpl::kGraphSteps); // warm-up, including the first graph capture
+            t.finish();
+            cudaEvent_t e0, e1;
+            U3DG_CUDA(cudaEventCreate(&e0));
+            U3DG_CUDA(cudaEventCreate(&e1));
+            U3DG_CUDA(cudaEventRecord(e0, t.stream));
+            t.stepTo(t.iteration + 2 * TrainerImpl::kGraphSteps);
+            t.finish();
+            U3DG_CUDA(cudaEventRecord(e1, t.stream));
+            U3DG_CUDA(cudaEventSynchronize(e1));
+            U3DG_CUDA(cudaEventElapsedTime(&stepMs[d], e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            stepMs[d] /= float(2 * TrainerImpl::kGraphSteps);
+            t.timer = new PhaseTimer();
+            t.profiling = true;
+            t.stepTo(t.iteration + TrainerImpl::kGraphSteps);
+            t.sync();
+            const u3dg_phase_times &acc = t.timer->acc;
+            fwdMs[d] = acc.steps ? acc.forward_ms / float(acc.steps) : 0.0f;
+            bwdMs[d] = acc.steps ? acc.backward_ms / float(acc.steps) : 0.0f;
         }
+        const int fd = fwdMs[1] < fwdMs[0] ? 2 : 1, bd = bwdMs[1] < bwdMs[0] ? 2 : 1;
+        const float ms = stepMs[0] - (fwdMs[0] - fwdMs[fd - 1]) - (bwdMs[0] - bwdMs[bd - 1]);
+        // Tile 32 spans four CTAs per tile that add partial gradients atomically (run-to-run float
+        // differences); it has to be clearly faster than the deterministic sizes to be chosen. The
+        // batch depths change no result.
+        const float need = tile > 16 ? 0.97f : 1.0f;
+        if (best.msPerStep == 0.0f || ms < need * best.msPerStep)
+            best = RasterSchedule{tile, fd, bd, ms};
     }
-    if (msPerStep)
-        *msPerStep = bestMs;
     return best;
 }
 

@@ -128,6 +128,8 @@ struct RasterArgs {
     int blocksX, blocksY;
     const int *blockOrder; // pixel blocks, heaviest tile list first (launchBlockOrder)
     int *counters;         // 4 ints, zero between launches: forward [0..1], backward [2..3]
+    int forwardDepth;      // list entries staged per thread per batch, forward: 1 or 2 (same results)
+    int backwardDepth;     // the same for the backward kernel
 };
 // Orders the pixel blocks by the list length of their tile, longest first (log-scale buckets), into
 // order[blocksX * blocksY].

@@ -45,13 +45,13 @@ __device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const fl
     last = lastIdx;
 }
 
-template <int PB>
+template <int PB, int BD>
 __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by, float *rgb, float *finalT,
                                              int *nContrib, float4 *sP, float4 *sQ, float4 *sR,
-                                             uint32_t (*mask)[RasterShape<PB>::NW])
+                                             uint32_t (*mask)[RasterShape<PB, BD>::NG])
 {
-    using S = RasterShape<PB>;
-    constexpr int NT = S::NT, NW = S::NW;
+    using S = RasterShape<PB, BD>;
+    constexpr int NT = S::NT, NB = S::NB, NG = S::NG;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const WarpBlock<PB> wb(warp, lane, bx, by);
     const int tile = tileOf<PB>(a, bx, by);
@@ -64,12 +64,16 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
     const float fx = float(wb.px), fy0 = float(wb.py0), fy1 = float(wb.py1);
     const float minA = a.minAlpha, minT = a.minTransmittance;
     const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
-    for (int b0 = start; b0 < end; b0 += NT) {
+    for (int b0 = start; b0 < end; b0 += NB) {
         if (__syncthreads_count(done0 && done1) == NT)
             break;
-        stage<PB>(rec, a.list, b0 + tid, b0 + tid < end, tid, sP, sQ, sR, mask, bx, by);
+#pragma unroll
+        for (int r = 0; r < BD; ++r) {
+            const int slot = r * NT + tid;
+            stage<PB, BD>(rec, a.list, b0 + slot, b0 + slot < end, slot, sP, sQ, sR, mask, bx, by);
+        }
         __syncthreads();
-        for (int k = 0; k < NW && !(done0 && done1); ++k) {
+        for (int k = 0; k < NG && !(done0 && done1); ++k) {
             uint32_t bits = mask[warp][k];
             while (bits) {
                 const int j = 32 * k + __ffs(bits) - 1;
@@ -110,25 +114,25 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
 #define U3DG_FWD_MIN_BLOCKS 10
 #endif
 
-template <int PB>
+template <int PB, int BD>
 __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_FWD_MIN_BLOCKS) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
                                                                               int *nContrib)
 {
-    using S = RasterShape<PB>;
-    constexpr int NT = S::NT, NW = S::NW;
-    __shared__ float4 sP[NT]; // mx, my, ex, ey
-    __shared__ float4 sQ[NT]; // A, B, C, alpha
-    __shared__ float4 sR[NT]; // r, g, b, depth
-    __shared__ uint32_t mask[NW][NW];
+    using S = RasterShape<PB, BD>;
+    constexpr int NB = S::NB, NW = S::NW, NG = S::NG;
+    __shared__ float4 sP[NB]; // mx, my, powMin, ey
+    __shared__ float4 sQ[NB]; // A, B, C, alpha
+    __shared__ float4 sR[NB]; // r, g, b, powMin
+    __shared__ uint32_t mask[NW][NG];
     __shared__ int sNext;
     const int units = a.blocksX * a.blocksY;
     if (a.counters == nullptr) { // one CTA per pixel block (every block resident in one wave)
-        forwardBlock<PB>(a, int(blockIdx.x) % a.blocksX, int(blockIdx.x) / a.blocksX, rgb, finalT, nContrib, sP, sQ,
-                         sR, mask);
+        forwardBlock<PB, BD>(a, int(blockIdx.x) % a.blocksX, int(blockIdx.x) / a.blocksX, rgb, finalT, nContrib, sP,
+                             sQ, sR, mask);
         return;
     }
     for (int b = nextBlock(a, a.counters, &sNext); b < units; b = nextBlock(a, a.counters, &sNext))
-        forwardBlock<PB>(a, b % a.blocksX, b / a.blocksX, rgb, finalT, nContrib, sP, sQ, sR, mask);
+        forwardBlock<PB, BD>(a, b % a.blocksX, b / a.blocksX, rgb, finalT, nContrib, sP, sQ, sR, mask);
 }
 
 // One CTA: the pixel blocks bucketed by the list length of their tile on a log scale (four buckets
@@ -198,25 +202,28 @@ void launchBlockOrder(const RasterArgs &a, int *order, cudaStream_t s)
     { blockOrderKernel<<<1, 1024, 0, s>>>(a.tileOffsets, a.blocksX, a.blocksY, pb, a.tileSize, a.tilesX, order); countLaunch(); }
 }
 
-void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
+template <int PB, int BD>
+static void launchForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
 {
-    const int units = a.blocksX * a.blocksY;
-    if (units <= 0)
-        return;
     // When every pixel block fits on the GPU at once, one CTA per block in natural order (no work
     // counter); otherwise the persistent schedule on counters[0..1].
+    const int units = a.blocksX * a.blocksY;
+    static const int ctas = residentCtas(compositeForwardKernel<PB, BD>, RasterShape<PB>::NT, 0);
     RasterArgs f = a;
-    if (a.tileSize <= 8) {
-        static const int ctas = residentCtas(compositeForwardKernel<8>, RasterShape<8>::NT, 0);
-        if (units <= ctas)
-            f.counters = nullptr;
-        { compositeForwardKernel<8><<<std::min(units, ctas), RasterShape<8>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
-    } else {
-        static const int ctas = residentCtas(compositeForwardKernel<16>, RasterShape<16>::NT, 0);
-        if (units <= ctas)
-            f.counters = nullptr;
-        { compositeForwardKernel<16><<<std::min(units, ctas), RasterShape<16>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
-    }
+    if (units <= ctas)
+        f.counters = nullptr;
+    { compositeForwardKernel<PB, BD><<<std::min(units, ctas), RasterShape<PB>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
+}
+
+void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
+{
+    if (a.blocksX * a.blocksY <= 0)
+        return;
+    const bool deep = a.forwardDepth >= 2;
+    if (a.tileSize <= 8)
+        deep ? launchForward<8, 2>(a, rgb, finalT, nContrib, s) : launchForward<8, 1>(a, rgb, finalT, nContrib, s);
+    else
+        deep ? launchForward<16, 2>(a, rgb, finalT, nContrib, s) : launchForward<16, 1>(a, rgb, finalT, nContrib, s);
 }
 
 } // namespace u3dg

@@ -141,14 +141,14 @@ __device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix
     s.fy = fy;
 }
 
-template <int PB>
+template <int PB, int BD>
 __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int by, const float *dLdRgb,
                                               const float *finalTIn, const int *nContribIn, float *partial,
                                               int useAtomics, float4 *sP, float4 *sQ, float4 *sR,
-                                              uint32_t (*mask)[RasterShape<PB>::NW], int &sMax, float *sWarp)
+                                              uint32_t (*mask)[RasterShape<PB, BD>::NG], int &sMax, float *sWarp)
 {
-    using S = RasterShape<PB>;
-    constexpr int NT = S::NT, NW = S::NW;
+    using S = RasterShape<PB, BD>;
+    constexpr int NT = S::NT, NW = S::NW, NB = S::NB, NG = S::NG;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const WarpBlock<PB> wb(warp, lane, bx, by);
     const int tile = tileOf<PB>(a, bx, by);
@@ -181,18 +181,22 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
             for (int k = 0; k < kG2d; ++k)
                 dst[k] = 0.0f;
         }
-    float *myWarp = sWarp + size_t(warp) * NT * kG2d;
-    for (int bEnd = jmax; bEnd > 0; bEnd -= NT) {
-        const int bStart = max(0, bEnd - NT), cnt = bEnd - bStart;
+    float *myWarp = sWarp + size_t(warp) * NB * kG2d;
+    for (int bEnd = jmax; bEnd > 0; bEnd -= NB) {
+        const int bStart = max(0, bEnd - NB), cnt = bEnd - bStart;
         __syncthreads();
-        stage<PB>(rec, a.list, start + bStart + tid, tid < cnt, tid, sP, sQ, sR, mask, bx, by);
+#pragma unroll
+        for (int r = 0; r < BD; ++r) {
+            const int slot = r * NT + tid;
+            stage<PB, BD>(rec, a.list, start + bStart + slot, slot < cnt, slot, sP, sQ, sR, mask, bx, by);
+        }
         {
             float4 *z = reinterpret_cast<float4 *>(sWarp);
-            for (int k = tid; k < NW * NT * kG2d / 4; k += NT)
+            for (int k = tid; k < NW * NB * kG2d / 4; k += NT)
                 z[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         __syncthreads();
-        for (int k = NW - 1; k >= 0; --k) {
+        for (int k = NG - 1; k >= 0; --k) {
             uint32_t bits = mask[warp][k];
             const int lim = wMax - bStart - 32 * k; // entries of this group below wMax
             if (lim <= 0)
@@ -229,17 +233,21 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
             }
         }
         __syncthreads();
-        if (tid < cnt) {
+#pragma unroll
+        for (int r = 0; r < BD; ++r) {
+            const int e = r * NT + tid;
+            if (e >= cnt)
+                break;
             float sum[kG2d];
 #pragma unroll
             for (int q = 0; q < kG2d; ++q)
-                sum[q] = sWarp[tid * kG2d + q];
+                sum[q] = sWarp[e * kG2d + q];
             for (int w = 1; w < NW; ++w)
 #pragma unroll
                 for (int q = 0; q < kG2d; ++q)
-                    sum[q] += sWarp[(size_t(w) * NT + tid) * kG2d + q];
-            finishEntry(sQ[tid], sum);
-            float *dst = partial + size_t(a.listEmit[start + bStart + tid]) * kG2d;
+                    sum[q] += sWarp[(size_t(w) * NB + e) * kG2d + q];
+            finishEntry(sQ[e], sum);
+            float *dst = partial + size_t(a.listEmit[start + bStart + e]) * kG2d;
             if (useAtomics) {
 #pragma unroll
                 for (int q = 0; q < kG2d; ++q)
@@ -264,25 +272,25 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
 #define U3DG_BWD_CARVEOUT -1
 #endif
 
-template <int PB>
+template <int PB, int BD>
 __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
                                                                               const float *finalTIn,
                                                                               const int *nContribIn, float *partial,
                                                                               int useAtomics)
 {
-    using S = RasterShape<PB>;
-    constexpr int NT = S::NT, NW = S::NW;
-    __shared__ float4 sP[NT];
-    __shared__ float4 sQ[NT];
-    __shared__ float4 sR[NT];
-    __shared__ uint32_t mask[NW][NW];
+    using S = RasterShape<PB, BD>;
+    constexpr int NB = S::NB, NW = S::NW, NG = S::NG;
+    __shared__ float4 sP[NB];
+    __shared__ float4 sQ[NB];
+    __shared__ float4 sR[NB];
+    __shared__ uint32_t mask[NW][NG];
     __shared__ int sMax, sNext;
-    extern __shared__ float sWarp[]; // NW slots of NT entries x 9 sums
+    extern __shared__ float sWarp[]; // NW slots of NB entries x 9 sums
     const int units = a.blocksX * a.blocksY;
     int *counter = a.counters + 2; // backward: counters[2..3]
     for (int b = nextBlock(a, counter, &sNext); b < units; b = nextBlock(a, counter, &sNext))
-        backwardBlock<PB>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, useAtomics, sP, sQ,
-                          sR, mask, sMax, sWarp);
+        backwardBlock<PB, BD>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, useAtomics, sP,
+                              sQ, sR, mask, sMax, sWarp);
 }
 
 template <class K>
@@ -299,23 +307,33 @@ int residentCtas(K kernel, int threads, size_t smem)
 
 } // namespace
 
+template <int PB, int BD>
+static void launchBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
+                           float *partial, cudaStream_t s)
+{
+    using S = RasterShape<PB, BD>;
+    const size_t smem = size_t(S::NW) * S::NB * kG2d * sizeof(float); // 18 KB (BD 1) or 36 KB (BD 2) at PB 16
+    static const int ctas = [&] {
+        cudaFuncSetAttribute(compositeBackwardKernel<PB, BD>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        return residentCtas(compositeBackwardKernel<PB, BD>, S::NT, smem);
+    }();
+    const int units = a.blocksX * a.blocksY;
+    { compositeBackwardKernel<PB, BD><<<std::min(units, ctas), S::NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial,
+                                                                          a.tileSize > PB ? 1 : 0); countLaunch(); }
+}
+
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
                              float *partial, cudaStream_t s)
 {
-    const int units = a.blocksX * a.blocksY;
-    if (units <= 0)
+    if (a.blocksX * a.blocksY <= 0)
         return;
-    if (a.tileSize <= 8) {
-        constexpr int NT = RasterShape<8>::NT, NW = RasterShape<8>::NW;
-        const size_t smem = size_t(NW) * NT * kG2d * sizeof(float);
-        static const int ctas = residentCtas(compositeBackwardKernel<8>, NT, smem);
-        { compositeBackwardKernel<8><<<std::min(units, ctas), NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, 0); countLaunch(); }
-    } else {
-        constexpr int NT = RasterShape<16>::NT, NW = RasterShape<16>::NW;
-        const size_t smem = size_t(NW) * NT * kG2d * sizeof(float); // 18 KB: no opt-in needed
-        static const int ctas = residentCtas(compositeBackwardKernel<16>, NT, smem);
-        { compositeBackwardKernel<16><<<std::min(units, ctas), NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial, a.tileSize > 16 ? 1 : 0); countLaunch(); }
-    }
+    const bool deep = a.backwardDepth >= 2;
+    if (a.tileSize <= 8)
+        deep ? launchBackward<8, 2>(a, dLdRgb, finalT, nContrib, partial, s)
+             : launchBackward<8, 1>(a, dLdRgb, finalT, nContrib, partial, s);
+    else
+        deep ? launchBackward<16, 2>(a, dLdRgb, finalT, nContrib, partial, s)
+             : launchBackward<16, 1>(a, dLdRgb, finalT, nContrib, partial, s);
 }
 
 } // namespace u3dg

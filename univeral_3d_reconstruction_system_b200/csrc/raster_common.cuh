@@ -2,20 +2,24 @@
 //
 // A CTA covers a PB x PB pixel block (PB = 16, or 8 for tile size 8) with PB*PB/2 threads; a warp
 // owns an 8 x 8 pixel block and each thread two pixels of the same column, rows r and r + 4. A tile's
-// depth-sorted list is walked in batches of one record per thread; while staging a batch, warp k votes
-// which of its 32 entries meet each warp's pixel block (the Gaussian's conservative contributing box,
-// SplatRec::ex / ey, against the block), so each warp later walks only the set bits of its mask.
+// depth-sorted list is walked in batches of BD records per thread (the batch depth, 1 or 2); while
+// staging a batch, each warp votes which of its 32 entries meet each warp's pixel block (the Gaussian's
+// conservative contributing box, SplatRec::ex / ey, against the block), so each warp later walks only
+// the set bits of its mask. The batch depth changes how many entries are staged per barrier, not any
+// result: every entry is evaluated the same way in the same order.
 #pragma once
 
 #include "kernels.h"
 
 namespace u3dg {
 
-template <int PB>
+template <int PB, int BD = 1>
 struct RasterShape {
-    static constexpr int NT = PB * PB / 2; // threads = batch entries
+    static constexpr int NT = PB * PB / 2; // threads
     static constexpr int NW = NT / 32;     // warps
     static constexpr int WX = PB / 8;      // warp blocks per row
+    static constexpr int NB = NT * BD;     // batch entries
+    static constexpr int NG = NB / 32;     // 32-entry groups of a batch (mask words per warp)
 };
 
 // This thread's two pixels and its warp's 8x8 block, in pixel block (bx, by).
@@ -76,12 +80,13 @@ __device__ __forceinline__ int nextBlock(const RasterArgs &a, int *counter, int 
     return u < units ? a.blockOrder[u] : units;
 }
 
-// Stages batch entry `slot` (if valid) and the masks: mask[w][k] bit b <=> entry 32k + b meets warp w.
-template <int PB>
+// Stages batch entry `slot` (if valid) and the masks: mask[w][g] bit b <=> entry 32g + b meets warp w.
+template <int PB, int BD>
 __device__ __forceinline__ void stage(const float4 *rec, const int *list, int idx, bool valid, int slot, float4 *sP,
-                                      float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB>::NW], int bx, int by)
+                                      float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB, BD>::NG], int bx,
+                                      int by)
 {
-    constexpr int NW = RasterShape<PB>::NW;
+    constexpr int NW = RasterShape<PB, BD>::NW;
     float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f);
     if (valid) {
         const float4 *r = rec + size_t(list[idx]) * 3;
@@ -93,12 +98,12 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
         sQ[slot] = r[1];
         sR[slot] = c;
     }
-    const int warp = slot >> 5, lane = slot & 31;
+    const int group = slot >> 5, lane = slot & 31;
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
         const uint32_t bits = __ballot_sync(0xffffffffu, valid && meets<PB>(p, w, bx, by));
         if (lane == 0)
-            mask[w][warp] = bits;
+            mask[w][group] = bits;
     }
 }
 
