@@ -335,8 +335,8 @@ def run_ours(args, dist: Dist) -> dict:
 
 def run_batched(args, dist: Dist) -> dict:
     """Batched multi-scene training: 16 seeded scenes (scenes.batched_specs) trained together by one
-    u3dg_batch (per-scene streams, step graphs, tile sizes and compositing batch depths from the
-    autotuner), then each scene alone with its tuned tile size and batch depth. Reports the aggregate
+    u3dg_batch (per-scene streams, step graphs, tile sizes and compositing schedules from the
+    autotuner), then each scene alone with its tuned tile size and schedule. Reports the aggregate
     iterations/s of both and every scene's PSNR. With N ranks, rank r takes scenes r, r + N, ...
     (scenes are independent: no collective on the data path); the rates are total iterations over the
     slowest rank's time."""
@@ -364,17 +364,17 @@ def run_batched(args, dist: Dist) -> dict:
     rows = []
     seq_ms = 0.0
     for k, (init, imgs, extent, opt) in enumerate(scenes):
-        tile, fwd_depth, bwd_depth, tuned = b.schedule(k)
+        tile, raster, tuned = b.schedule(k)
         tb = b.trainer(k)
         p_batch = tb.evaluatePsnr()
         o2 = dataclasses.replace(opt, raster=dataclasses.replace(opt.raster, tile_size=tile))
         t = api.Trainer(init, imgs, extent, o2)
-        t.set_batch_depth(fwd_depth, bwd_depth)
+        t.set_raster_schedule(*raster)
         seq_ms += t.time_steps(opt.iterations)
         p_alone = t.evaluatePsnr()
         rows.append({"scene": specs[k].name, "gt": specs[k].gt_count, "views": specs[k].views,
                      "width": specs[k].width, "iterations": opt.iterations, "tile": tile,
-                     "batch_depths": [fwd_depth, bwd_depth],
+                     "raster_schedule": list(raster),
                      "tuned_ms_per_step": round(tuned, 4), "gaussians": tb.size(), "psnr_batched": round(p_batch, 4),
                      "psnr_alone": round(p_alone, 4)})
         t.close()

@@ -439,13 +439,16 @@ public:
         check(u3dg_batch_tile_size(m_b, scene, &t, nullptr));
         return t;
     }
-    // List entries each forward / backward compositing thread stages per batch (1 or 2), chosen with
-    // the tile size.
-    std::pair<int, int> batchDepths(int scene) const
+    // Compositing schedule chosen with the tile size: the forward kernel's pixel block edge and the
+    // list entries each forward / backward thread stages per batch (u3dg_trainer_set_raster_schedule).
+    struct RasterSchedule {
+        int forwardBlock, forwardDepth, backwardDepth;
+    };
+    RasterSchedule rasterSchedule(int scene) const
     {
-        int f = 0, b = 0;
-        check(u3dg_batch_schedule(m_b, scene, nullptr, &f, &b, nullptr));
-        return {f, b};
+        RasterSchedule r{};
+        check(u3dg_batch_schedule(m_b, scene, nullptr, &r.forwardBlock, &r.forwardDepth, &r.backwardDepth, nullptr));
+        return r;
     }
     // The scene's model, copied back from the GPU.
     GaussianModel model(int scene) const

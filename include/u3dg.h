@@ -209,11 +209,14 @@ int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms);
  * graph launches ran so far. */
 int u3dg_trainer_set_graphs(u3dg_trainer *trainer, int enable);
 int u3dg_trainer_graph_launches(u3dg_trainer *trainer, long long *launches);
-/* No reference counterpart. List entries each thread of the forward and of the backward compositing
- * kernel stages per shared-memory batch: 1 (default) or 2 each. Deeper batches halve the block
- * barriers per Gaussian at the cost of shared memory; the rendered images, gradients and trained
+/* No reference counterpart. Compositing schedule: forward_block is the pixel block edge of the
+ * forward kernel for tiles of 16 and 32 pixels, 8 (default: several 8x8 CTAs walk each tile list) or
+ * 16; forward_depth and backward_depth are the list entries each thread of the forward and of the
+ * backward kernel stages per shared-memory batch, 1 (default) or 2 (deeper batches halve the block
+ * barriers per Gaussian at the cost of shared memory). The rendered images, gradients and trained
  * models are bit-identical for every setting. */
-int u3dg_trainer_set_batch_depth(u3dg_trainer *trainer, int forward_depth, int backward_depth);
+int u3dg_trainer_set_raster_schedule(u3dg_trainer *trainer, int forward_block, int forward_depth,
+                                     int backward_depth);
 void u3dg_trainer_destroy(u3dg_trainer *trainer);
 
 /* ------------------------------------------------------------------ rasterizer (unit boundary) */
@@ -269,11 +272,10 @@ int u3dg_densify_and_prune(u3dg_model *model, u3dg_model *adam_m, u3dg_model *ad
  * and options[s] (each with its own schedule and Gaussian cap). Every scene keeps its own trainer and
  * stream; u3dg_batch_step advances each scene by `count` iterations (or to its end), interleaving the
  * scenes so their kernels run concurrently and running steps through each scene's step graph where
- * it can. With autotune != 0, each scene's tile size (8, 16 or 32) and the batch depths of its
- * forward and backward compositing kernels (1 or 2 list entries staged per thread per batch; same
- * results either way) are chosen at creation from short timed runs on throwaway trainers; tile_size
- * reports the tile and the tuned ms per step (0 without autotune), schedule the depths as well.
- * batch_trainer
+ * it can. With autotune != 0, each scene's tile size (8, 16 or 32) and compositing schedule (the
+ * settings of u3dg_trainer_set_raster_schedule; same results for any) are chosen at creation from
+ * short timed runs on throwaway trainers; tile_size reports the tile and the tuned ms per step (0
+ * without autotune), schedule the compositing settings as well. batch_trainer
  * returns a borrowed handle for the per-scene queries of the u3dg_trainer_* API (download, stats,
  * eval_psnr, ...); destroying it is a no-op, the batch owns it. time_steps steps like batch_step and
  * reports the device time from one event that all scene streams wait on to the last stream's end. */
@@ -286,8 +288,8 @@ int u3dg_batch_time_steps(u3dg_batch *batch, int count, float *ms);
 int u3dg_batch_size(u3dg_batch *batch, int *scenes);
 int u3dg_batch_trainer(u3dg_batch *batch, int scene, u3dg_trainer **out);
 int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_ms_per_step);
-int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_depth, int *backward_depth,
-                        float *tuned_ms_per_step);
+int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_block, int *forward_depth,
+                        int *backward_depth, float *tuned_ms_per_step);
 /* Rounds in which every unfinished scene ran its next 10 steps as one CUDA graph launch holding all
  * scenes (scenes whose buffers stayed put since the previous round), and how often that graph was
  * recorded. Either pointer may be NULL. */

@@ -1,5 +1,5 @@
 """Batched multi-scene training (u3dg_batch_*): every scene of a batch trains exactly as the same scene
-trained alone, with or without the autotuner of tile size and compositing batch depth."""
+trained alone, with or without the autotuner of tile size and compositing schedule."""
 from __future__ import annotations
 
 import dataclasses
@@ -27,11 +27,11 @@ def _scenes(u3dg):
     return out
 
 
-def _alone(u3dg, scene, tile, depths, iterations):
+def _alone(u3dg, scene, tile, raster, iterations):
     init, imgs, extent, opt = scene
     opt = dataclasses.replace(opt, raster=dataclasses.replace(opt.raster, tile_size=tile))
     t = u3dg.Trainer(init, imgs, extent, opt)
-    t.set_batch_depth(*depths)
+    t.set_raster_schedule(*raster)
     t.step(iterations)
     return t.model().flat(), t.stats()
 
@@ -49,16 +49,16 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
     assert launches >= 3 and 1 <= captures <= launches
     for k, scene in enumerate(scenes):
         tile, tuned = b.tile_size(k)
-        tile2, fd, bd, tuned2 = b.schedule(k)
+        tile2, raster, tuned2 = b.schedule(k)
         assert (tile2, tuned2) == (tile, tuned)
-        assert tile in (8, 16, 32) and fd in (1, 2) and bd in (1, 2)
+        assert tile in (8, 16, 32) and raster[0] in (8, 16) and raster[1] in (1, 2) and raster[2] in (1, 2)
         if not autotune:
-            assert (tile, fd, bd, tuned) == (16, 1, 1, 0.0)
+            assert (tile, raster, tuned) == (16, (8, 1, 1), 0.0)
         else:
             assert tuned > 0
         t = b.trainer(k)
         assert t.iteration() == 250
-        flat, st = _alone(u3dg, scene, tile, (fd, bd), 250)
+        flat, st = _alone(u3dg, scene, tile, raster, 250)
         got = t.model().flat()
         if tile == 32:
             # Tiles of 32 pixels span four CTAs that add their partial gradients atomically: the same

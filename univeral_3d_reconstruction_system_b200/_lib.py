@@ -60,7 +60,7 @@ SIGNATURES = {
     "u3dg_trainer_replays": (C.c_int, [_P, _I]),
     "u3dg_trainer_set_graphs": (C.c_int, [_P, C.c_int]),
     "u3dg_trainer_graph_launches": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
-    "u3dg_trainer_set_batch_depth": (C.c_int, [_P, C.c_int, C.c_int]),
+    "u3dg_trainer_set_raster_schedule": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     "u3dg_trainer_destroy": (None, [_P]),
     "u3dg_rasterizer_create": (C.c_int, [_PP]),
     "u3dg_rasterizer_forward": (C.c_int, [_P, _MV, _CAM, _ST, _F]),
@@ -79,7 +79,7 @@ SIGNATURES = {
     "u3dg_batch_size": (C.c_int, [_P, _I]),
     "u3dg_batch_trainer": (C.c_int, [_P, C.c_int, _PP]),
     "u3dg_batch_tile_size": (C.c_int, [_P, C.c_int, _I, _F]),
-    "u3dg_batch_schedule": (C.c_int, [_P, C.c_int, _I, _I, _I, _F]),
+    "u3dg_batch_schedule": (C.c_int, [_P, C.c_int, _I, _I, _I, _I, _F]),
     "u3dg_batch_graph_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "u3dg_batch_destroy": (None, [_P]),
     "u3dg_photometric_loss": (C.c_int, [_F, _F, C.c_int, C.c_int, C.c_float, _F, C.POINTER(_abi.LossValue)]),

@@ -136,10 +136,11 @@ class Trainer:
         check(load().u3dg_trainer_graph_launches(self._h, C.byref(v)))
         return int(v.value)
 
-    def set_batch_depth(self, forward: int, backward: int | None = None) -> None:
-        """List entries staged per thread per batch by the forward and backward compositing kernels,
-        1 or 2 each (identical results); backward defaults to forward."""
-        check(load().u3dg_trainer_set_batch_depth(self._h, forward, forward if backward is None else backward))
+    def set_raster_schedule(self, forward_block: int = 8, forward_depth: int = 1, backward_depth: int = 1) -> None:
+        """Compositing schedule (identical results for every setting): the forward kernel's pixel block
+        edge for tiles of 16 and 32 pixels (8 or 16) and the list entries each forward / backward
+        thread stages per shared-memory batch (1 or 2)."""
+        check(load().u3dg_trainer_set_raster_schedule(self._h, forward_block, forward_depth, backward_depth))
 
     def set_profiling(self, enable: bool) -> None:
         check(load().u3dg_trainer_set_profiling(self._h, 1 if enable else 0))
@@ -214,10 +215,12 @@ class Batch:
         return int(tile.value), float(ms.value)
 
     def schedule(self, scene: int):
-        """(tile size, forward batch depth, backward batch depth, tuned ms per step) of a scene."""
-        tile, fd, bd, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
-        check(load().u3dg_batch_schedule(self._h, scene, C.byref(tile), C.byref(fd), C.byref(bd), C.byref(ms)))
-        return int(tile.value), int(fd.value), int(bd.value), float(ms.value)
+        """(tile size, (forward block, forward depth, backward depth), tuned ms per step) of a scene;
+        the middle triple is the argument list of Trainer.set_raster_schedule."""
+        tile, fb, fd, bd, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+        check(load().u3dg_batch_schedule(self._h, scene, C.byref(tile), C.byref(fb), C.byref(fd), C.byref(bd),
+                                         C.byref(ms)))
+        return int(tile.value), (int(fb.value), int(fd.value), int(bd.value)), float(ms.value)
 
     def graph_launches(self):
         """(rounds run as one graph launch holding every scene, recordings of that graph)."""

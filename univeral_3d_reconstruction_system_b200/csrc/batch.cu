@@ -66,12 +66,13 @@ int u3dg_batch_create(const u3dg_model *initial, const u3dg_image *const *images
                                          !initial[s].opacities || !initial[s].colors))
                 throw StatusError(U3DG_ERR_INVALID_ARG, "scene " + std::to_string(s) + ": model has NULL arrays");
             u3dg_train_options o = options[s];
-            RasterSchedule rs{o.raster.tile_size, 1, 1, 0.0f};
+            RasterSchedule rs{o.raster.tile_size, 8, 1, 1, 0.0f};
             if (autotune)
                 rs = autotuneSchedule(initial[s], images[s], image_counts[s], extents[s], options[s]);
             o.raster.tile_size = rs.tileSize;
             auto t = std::make_unique<u3dg_trainer>();
             t->impl = std::make_unique<TrainerImpl>(initial[s], images[s], image_counts[s], extents[s], o);
+            t->impl->ws.forwardBlock = rs.forwardBlock;
             t->impl->ws.forwardDepth = rs.forwardDepth;
             t->impl->ws.backwardDepth = rs.backwardDepth;
             t->ownedByBatch = true;
@@ -151,11 +152,11 @@ int u3dg_batch_trainer(u3dg_batch *batch, int scene, u3dg_trainer **out)
 
 int u3dg_batch_tile_size(u3dg_batch *batch, int scene, int *tile, float *tuned_ms_per_step)
 {
-    return u3dg_batch_schedule(batch, scene, tile, nullptr, nullptr, tuned_ms_per_step);
+    return u3dg_batch_schedule(batch, scene, tile, nullptr, nullptr, nullptr, tuned_ms_per_step);
 }
 
-int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_depth, int *backward_depth,
-                        float *tuned_ms_per_step)
+int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_block, int *forward_depth,
+                        int *backward_depth, float *tuned_ms_per_step)
 {
     return guardedCall([&] {
         u3dg_batch &b = batchOf(batch);
@@ -163,6 +164,8 @@ int u3dg_batch_schedule(u3dg_batch *batch, int scene, int *tile, int *forward_de
         const RasterSchedule &rs = b.schedules[size_t(scene)];
         if (tile)
             *tile = rs.tileSize;
+        if (forward_block)
+            *forward_block = rs.forwardBlock;
         if (forward_depth)
             *forward_depth = rs.forwardDepth;
         if (backward_depth)

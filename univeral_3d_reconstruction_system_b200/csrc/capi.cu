@@ -367,14 +367,18 @@ int u3dg_trainer_set_graphs(u3dg_trainer *trainer, int enable)
     });
 }
 
-int u3dg_trainer_set_batch_depth(u3dg_trainer *trainer, int forward_depth, int backward_depth)
+int u3dg_trainer_set_raster_schedule(u3dg_trainer *trainer, int forward_block, int forward_depth,
+                                     int backward_depth)
 {
     return guarded([&] {
         TrainerImpl &t = impl(trainer);
+        if (forward_block != 8 && forward_block != 16)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "forward block must be 8 or 16");
         for (int d : {forward_depth, backward_depth})
             if (d != 1 && d != 2)
                 throw StatusError(U3DG_ERR_INVALID_ARG, "batch depth must be 1 or 2");
         t.finish();
+        t.ws.forwardBlock = forward_block;
         t.ws.forwardDepth = forward_depth;
         t.ws.backwardDepth = backward_depth;
         t.stepGraph.reset(); // its kernels were recorded for the other depth

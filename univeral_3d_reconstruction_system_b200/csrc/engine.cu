@@ -210,6 +210,7 @@ RasterArgs RasterWorkspace::rasterArgs() const
     a.blocksY = (cam.height + pb - 1) / pb;
     a.blockOrder = blockOrder.p;
     a.counters = blockCounters.p;
+    a.forwardBlock = forwardBlock;
     a.forwardDepth = forwardDepth;
     a.backwardDepth = backwardDepth;
     return a;
@@ -888,17 +889,20 @@ RasterSchedule autotuneSchedule(const u3dg_model &initial, const u3dg_image *img
                                 const u3dg_train_options &opt)
 {
     static const int kTiles[3] = {16, 8, 32};
-    RasterSchedule best{opt.raster.tile_size, 1, 1, 0.0f};
+    RasterSchedule best{opt.raster.tile_size, 8, 1, 1, 0.0f};
     for (int tile : kTiles) {
-        // Per depth: the step time of graph runs, then the compositing kernels' share from profiled
-        // steps. The forward and backward depths are picked independently (the kernels do not interact),
-        // and the tile's step time is that of depth 1 corrected by the gains of the picked depths.
+        // Two runs per tile: forward 16x16 blocks at depth 1 with the backward at depth 1, and forward
+        // 8x8 blocks at depth 2 with the backward at depth 2 (tile 8: both forwards use 8x8 blocks, at
+        // depth 1 and 2). Each times graph runs of whole steps, then profiled steps for the compositing
+        // kernels' own times; the forward and backward settings are picked independently (the kernels
+        // do not interact) and the tile's step time is the first run's corrected by their gains.
         float stepMs[2] = {}, fwdMs[2] = {}, bwdMs[2] = {};
         for (int d = 0; d < 2; ++d) {
             u3dg_train_options o = opt;
             o.raster.tile_size = tile;
             o.iterations = std::max(o.iterations, 64);
             TrainerImpl t(initial, imgs, count, extent, o);
+            t.ws.forwardBlock = d == 0 ? 16 : 8;
             t.ws.forwardDepth = t.ws.backwardDepth = d + 1;
             t.stepTo(3 + TrainerImpl::kGraphSteps); // warm-up, including the first graph capture
             t.finish();
@@ -922,14 +926,14 @@ RasterSchedule autotuneSchedule(const u3dg_model &initial, const u3dg_image *img
             fwdMs[d] = acc.steps ? acc.forward_ms / float(acc.steps) : 0.0f;
             bwdMs[d] = acc.steps ? acc.backward_ms / float(acc.steps) : 0.0f;
         }
-        const int fd = fwdMs[1] < fwdMs[0] ? 2 : 1, bd = bwdMs[1] < bwdMs[0] ? 2 : 1;
-        const float ms = stepMs[0] - (fwdMs[0] - fwdMs[fd - 1]) - (bwdMs[0] - bwdMs[bd - 1]);
+        const int f = fwdMs[1] < fwdMs[0] ? 1 : 0, b = bwdMs[1] < bwdMs[0] ? 1 : 0;
+        const float ms = stepMs[0] - (fwdMs[0] - fwdMs[f]) - (bwdMs[0] - bwdMs[b]);
         // Tile 32 spans four CTAs per tile that add partial gradients atomically (run-to-run float
         // differences); it has to be clearly faster than the deterministic sizes to be chosen. The
-        // batch depths change no result.
+        // other settings change no result.
         const float need = tile > 16 ? 0.97f : 1.0f;
         if (best.msPerStep == 0.0f || ms < need * best.msPerStep)
-            best = RasterSchedule{tile, fd, bd, ms};
+            best = RasterSchedule{tile, f == 0 && tile > 8 ? 16 : 8, f + 1, b + 1, ms};
     }
     return best;
 }

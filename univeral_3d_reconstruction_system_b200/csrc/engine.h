@@ -161,8 +161,10 @@ struct RasterWorkspace {
     HostPinned<BinCounts> hostCounts;
 
     int n = 0, tilesX = 0, tilesY = 0;
-    // Compositing: list entries staged per thread per shared-memory batch (1 or 2; same results).
-    int forwardDepth = 1, backwardDepth = 1;
+    // Compositing schedule (none changes a result): the forward kernel's pixel block edge (8 or 16,
+    // for tiles of 16 and 32 pixels) and the list entries each compositing thread stages per
+    // shared-memory batch (1 or 2).
+    int forwardBlock = 8, forwardDepth = 1, backwardDepth = 1;
     u3dg_camera cam{};
     u3dg_raster_settings st{};
     uint32_t *sortedIds = nullptr;
@@ -412,12 +414,12 @@ struct BatchGraph {
 // graph holding all of their chunks (bg, may be null: no combined graph).
 void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph *bg = nullptr);
 
-// Tile size (8, 16 or 32) and compositing batch depths (1 or 2 staged list entries per thread per
-// batch, for the forward and the backward kernel) with the shortest step time for a scene, timed on
-// throwaway trainers started from the same model. Tile 32, whose partial gradients are added
-// atomically, must be at least 3% faster than the best of 8 and 16.
+// Tile size (8, 16 or 32), forward pixel block (8 or 16) and compositing batch depths (1 or 2 staged
+// list entries per thread per batch, for the forward and the backward kernel) with the shortest step
+// time for a scene, timed on throwaway trainers started from the same model. Tile 32, whose partial
+// gradients are added atomically, must be at least 3% faster than the best of 8 and 16.
 struct RasterSchedule {
-    int tileSize, forwardDepth, backwardDepth;
+    int tileSize, forwardBlock, forwardDepth, backwardDepth;
     float msPerStep;
 };
 RasterSchedule autotuneSchedule(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,

@@ -128,6 +128,7 @@ struct RasterArgs {
     int blocksX, blocksY;
     const int *blockOrder; // pixel blocks, heaviest tile list first (launchBlockOrder)
     int *counters;         // 4 ints, zero between launches: forward [0..1], backward [2..3]
+    int forwardBlock;      // pixel block edge of the forward kernel: 8 or 16 (tiles > 8 only; same results)
     int forwardDepth;      // list entries staged per thread per batch, forward: 1 or 2 (same results)
     int backwardDepth;     // the same for the backward kernel
 };

@@ -1,8 +1,10 @@
 // raster.cu - tile compositing forward (Rasterizer::forward, Rasterizer.cpp:281-329).
 //
-// Layout and staging in raster_common.cuh: a CTA per 16x16 pixel block, two pixels per thread, 8x8
-// pixels per warp, batches of one list entry per thread staged in shared memory with per-warp masks of
-// the entries whose contributing box meets the warp's block. Each warp walks its set bits in list
+// Layout and staging in raster_common.cuh: a CTA per 16x16 or 8x8 pixel block, two pixels per thread,
+// 8x8 pixels per warp, batches of one or two list entries per thread staged in shared memory with
+// per-warp masks of the entries whose contributing box meets the warp's block. A tile of 16 or 32
+// pixels may be covered by several 8x8 CTAs that each walk the whole tile list (RasterArgs::
+// forwardBlock): more, shorter CTAs keep the SMs busy while the heaviest tiles finish. Each warp walks its set bits in list
 // order and blends both of its pixels' columns, front to back, with the reference's cut-offs
 // (alpha <= 0.99, skip alpha < minAlpha, stop when T (1 - alpha) < minTransmittance). A CTA stops when
 // every pixel has terminated (__syncthreads_count). Skipped entries are exactly those the reference
@@ -215,12 +217,26 @@ static void launchForward(const RasterArgs &a, float *rgb, float *finalT, int *n
     { compositeForwardKernel<PB, BD><<<std::min(units, ctas), RasterShape<PB>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
 }
 
+// 8x8 CTAs over the lists of larger tiles: one CTA per pixel block in natural order, as many waves as
+// it takes (the blocks are short; the persistent order is computed for the backward's blocks).
+template <int BD>
+static void launchForwardSplit(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
+{
+    RasterArgs f = a;
+    f.blocksX = (a.width + 7) / 8;
+    f.blocksY = (a.height + 7) / 8;
+    f.counters = nullptr;
+    { compositeForwardKernel<8, BD><<<f.blocksX * f.blocksY, RasterShape<8>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
+}
+
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)
 {
     if (a.blocksX * a.blocksY <= 0)
         return;
     const bool deep = a.forwardDepth >= 2;
-    if (a.tileSize <= 8)
+    if (a.tileSize > 8 && a.forwardBlock == 8)
+        deep ? launchForwardSplit<2>(a, rgb, finalT, nContrib, s) : launchForwardSplit<1>(a, rgb, finalT, nContrib, s);
+    else if (a.tileSize <= 8)
         deep ? launchForward<8, 2>(a, rgb, finalT, nContrib, s) : launchForward<8, 1>(a, rgb, finalT, nContrib, s);
     else
         deep ? launchForward<16, 2>(a, rgb, finalT, nContrib, s) : launchForward<16, 1>(a, rgb, finalT, nContrib, s);
