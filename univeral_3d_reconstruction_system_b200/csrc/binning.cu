@@ -402,7 +402,8 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
     const uint32_t *vin = nullptr;
     const int G = radixBlocks(nMax);
-    // Keys of up to 11 bits (tile ids) in one pass of 2048 digits; longer keys in 8-bit passes.
+    // Keys of up to 11 bits (tile ids) in one pass of 2048 digits; longer keys in 8-bit passes (three
+    // 11-bit passes over 32-bit depth keys measured slower than four 8-bit ones).
     const bool wide = bits <= kWideBits;
     const int db = wide ? kWideBits : 8;
     int passes = 0;
