@@ -49,6 +49,33 @@ __device__ __forceinline__ bool meets(const float4 &p, int w, int bx, int by)
     return !(p.x + p.z < x0 || p.x - p.z > x0 + 7.0f || p.y + p.w < y0 || p.y - p.w > y0 + 7.0f);
 }
 
+// Whether the contributing ellipse of a staged entry, {d : A dx^2 + 2 B dx dy + C dy^2 <= -2 powMin}
+// (power >= powMin), can reach a pixel centre of the 8x8 block [x0, x0 + 7] x [y0, y0 + 7]: the
+// minimum of the quadratic over the block (zero if the block holds the mean, else on an edge, where it
+// is a 1D quadratic minimised at a clamped stationary point) against the threshold widened by 4% and
+// 1e-3. Rounding-explicit, so every kernel builds the same masks; conservative like the box extents,
+// which are infinite for covariances whose condition number exceeds 1e4 (nothing is culled then).
+// Rotated, elongated footprints meet far fewer 8x8 blocks than their axis-aligned boxes suggest.
+__device__ __forceinline__ bool ellipseMeets(float mx, float my, const float4 &q, float powMin, float iA, float iC,
+                                             float x0, float y0)
+{
+    const float X0 = __fsub_rn(x0, mx), X1 = __fadd_rn(X0, 7.0f);
+    const float Y0 = __fsub_rn(y0, my), Y1 = __fadd_rn(Y0, 7.0f);
+    if (X0 <= 0.0f && X1 >= 0.0f && Y0 <= 0.0f && Y1 >= 0.0f)
+        return true;
+    const float A = q.x, B = q.y, C = q.z;
+    auto quad = [&](float dx, float dy) {
+        const float cross = __fmul_rn(2.0f, __fmul_rn(__fmul_rn(B, dx), dy));
+        return __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(A, dx), dx), cross), __fmul_rn(__fmul_rn(C, dy), dy));
+    };
+    const float nbc = __fmul_rn(-B, iC), nba = __fmul_rn(-B, iA);
+    float m = quad(X0, fminf(fmaxf(__fmul_rn(nbc, X0), Y0), Y1));
+    m = fminf(m, quad(X1, fminf(fmaxf(__fmul_rn(nbc, X1), Y0), Y1)));
+    m = fminf(m, quad(fminf(fmaxf(__fmul_rn(nba, Y0), X0), X1), Y0));
+    m = fminf(m, quad(fminf(fmaxf(__fmul_rn(nba, Y1), X0), X1), Y1));
+    return m <= __fadd_rn(__fmul_rn(-2.08f, powMin), 1e-3f);
+}
+
 template <int PB>
 __device__ __forceinline__ int tileOf(const RasterArgs &a, int bx, int by)
 {
@@ -86,22 +113,33 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
                                       float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB, BD>::NG], int bx,
                                       int by)
 {
-    constexpr int NW = RasterShape<PB, BD>::NW;
-    float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f);
+    constexpr int NW = RasterShape<PB, BD>::NW, WX = RasterShape<PB, BD>::WX;
+    float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f), q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float powMin = 0.0f, iA = 0.0f, iC = 0.0f;
     if (valid) {
         const float4 *r = rec + size_t(list[idx]) * 3;
         p = r[0];
+        q = r[1];
         const float4 c = r[2];
         // The blending loops read the mean from sP and the exponent floor (SplatRec::powMin) from its
         // third slot; the contributing box is only needed for the masks below.
         sP[slot] = make_float4(p.x, p.y, c.w, p.w);
-        sQ[slot] = r[1];
+        sQ[slot] = q;
         sR[slot] = c;
+        powMin = c.w;
+        iA = __frcp_rn(q.x);
+        iC = __frcp_rn(q.z);
     }
+    // The ellipse test refines the box test where the box extents are finite (well-conditioned
+    // covariances and a positive minimum alpha).
+    const bool fine = p.z < __int_as_float(0x7f800000);
     const int group = slot >> 5, lane = slot & 31;
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
-        const uint32_t bits = __ballot_sync(0xffffffffu, valid && meets<PB>(p, w, bx, by));
+        bool hit = valid && meets<PB>(p, w, bx, by);
+        if (hit && fine)
+            hit = ellipseMeets(p.x, p.y, q, powMin, iA, iC, float(bx * PB + (w % WX) * 8), float(by * PB + (w / WX) * 8));
+        const uint32_t bits = __ballot_sync(0xffffffffu, hit);
         if (lane == 0)
             mask[w][group] = bits;
     }
