@@ -217,6 +217,10 @@ int u3dg_trainer_graph_launches(u3dg_trainer *trainer, long long *launches);
  * models are bit-identical for every setting. */
 int u3dg_trainer_set_raster_schedule(u3dg_trainer *trainer, int forward_block, int forward_depth,
                                      int backward_depth);
+/* No reference counterpart. Tile culling (on by default): a Gaussian is listed only in the tiles of
+ * its rectangle that its contributing ellipse (alpha >= min_alpha) can reach, with a conservative
+ * margin; the trained models are bit-identical with it on (1) or off (0). */
+int u3dg_trainer_set_tile_culling(u3dg_trainer *trainer, int enable);
 void u3dg_trainer_destroy(u3dg_trainer *trainer);
 
 /* ------------------------------------------------------------------ rasterizer (unit boundary) */

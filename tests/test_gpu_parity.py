@@ -470,6 +470,49 @@ def test_raster_schedule_changes_no_result(u3dg, oracle, tiny_scene, tile):
             t.set_raster_schedule(*bad)
 
 
+@pytest.mark.parametrize("tile", [16, 8])
+def test_tile_culling_changes_no_result(u3dg, oracle, tiny_scene, tile):
+    """Listing a Gaussian only in the tiles its contributing ellipse reaches (the trainers' default)
+    keeps the trajectory of the reference's rectangle lists: every image and per-entry gradient is
+    the same, and only the summation order of a Gaussian's per-tile partials (a fixed-shape scan over
+    list positions, which culling shifts) differs, so models agree to rounding. Checked through
+    densification and graph runs."""
+    sc = tiny_scene
+    init = oracle.init_from_points(sc.init_xyz, sc.init_rgb)
+    opt = sc.options()
+    opt.raster.tile_size = tile
+    runs = []
+    for cull in (False, True):
+        t = u3dg.Trainer(init, sc.images, sc.extent, opt)
+        t.set_tile_culling(cull)
+        t.step(143)
+        runs.append((t.model(), t.stats()))
+    a, b = runs[0][1], runs[1][1]
+    assert a.iteration == b.iteration
+    assert abs(a.psnr - b.psnr) < 0.02 and abs(a.loss - b.loss) < 1e-3 * a.loss
+    assert abs(a.gaussians - b.gaussians) <= max(2, a.gaussians // 100)
+    if a.gaussians == b.gaussians:
+        assert rel_l2(runs[0][0].means, runs[1][0].means) < 1e-3
+
+
+@pytest.mark.parametrize("tile", [16, 8, 32])
+def test_tile_culling_renders_identically(u3dg, tile):
+    """Images of strongly anisotropic, rotated Gaussians (axis ratios up to ~60) are bit-identical with
+    and without tile culling, at every tile size, on a ragged view."""
+    rng = np.random.default_rng(11)
+    m = random_model(4000, rng, 1.6, 4.0, 0.004, 0.25)
+    m.scales[:, 0] += np.log(rng.uniform(1.0, 8.0, m.size())).astype(np.float32)
+    cam = make_camera(203, 141, 160.0)
+    t = u3dg.Trainer(m, [TrainImage(cam, np.zeros((cam.height, cam.width, 3), np.float32))], 1.0,
+                     TrainOptions(raster=RasterSettings(tile_size=tile)))
+    out = []
+    for cull in (False, True):
+        t.set_tile_culling(cull)
+        out.append(t.render(cam))
+    assert out[0].max() > 0.1
+    np.testing.assert_array_equal(out[0], out[1])
+
+
 @pytest.mark.parametrize("tile", [16, 32])
 @pytest.mark.parametrize("depth", [1, 2])
 def test_forward_on_8x8_blocks_is_bit_exact(u3dg, tiny_scene, tile, depth):

@@ -61,6 +61,7 @@ SIGNATURES = {
     "u3dg_trainer_set_graphs": (C.c_int, [_P, C.c_int]),
     "u3dg_trainer_graph_launches": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "u3dg_trainer_set_raster_schedule": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    "u3dg_trainer_set_tile_culling": (C.c_int, [_P, C.c_int]),
     "u3dg_trainer_destroy": (None, [_P]),
     "u3dg_rasterizer_create": (C.c_int, [_PP]),
     "u3dg_rasterizer_forward": (C.c_int, [_P, _MV, _CAM, _ST, _F]),

@@ -142,6 +142,10 @@ class Trainer:
         thread stages per shared-memory batch (1 or 2)."""
         check(load().u3dg_trainer_set_raster_schedule(self._h, forward_block, forward_depth, backward_depth))
 
+    def set_tile_culling(self, enable: bool) -> None:
+        """List Gaussians only in tiles their contributing ellipse reaches (default on; same models)."""
+        check(load().u3dg_trainer_set_tile_culling(self._h, 1 if enable else 0))
+
     def set_profiling(self, enable: bool) -> None:
         check(load().u3dg_trainer_set_profiling(self._h, 1 if enable else 0))
 

@@ -280,8 +280,90 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
         out[n] = partial[B];
 }
 
-__global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt,
-                                 int *rankOf)
+// Tile culling (trainers): a Gaussian is listed only in the tiles of its rectangle that its
+// contributing ellipse {d : A dx^2 + 2 B dx dy + C dy^2 <= t} (power >= powMin) can reach. In one tile
+// row the reachable tiles are contiguous: the ellipse cut by the row's strip of pixel centres spans
+// [xL, xR] with xR(dy) = (-B dy + sqrt(A t - det dy^2)) / A concave in dy, so its maximum over the
+// strip is at the clamped dy of the ellipse's rightmost point (and xL's minimum symmetrically).
+// Rounding-explicit (the count and the emission kernels get the same spans) and conservative like
+// the compositing kernels' block masks: t widened by 4% + 1e-3 and the span by one pixel each side.
+// Dropping entries that reach no pixel of a tile changes no image and no per-entry gradient.
+struct CullShape {
+    float mx, my, B, det, at, iA, ymax, dyR; // dyR: dy of the rightmost point, (-B / C) xmax
+    int mode;                                // 0: whole rectangle, 1: no tile, 2: culled rows
+};
+
+__device__ __forceinline__ CullShape cullShape(const SplatRec *rec, int g)
+{
+    const float4 *r = reinterpret_cast<const float4 *>(rec) + size_t(g) * 3;
+    const float4 p = r[0], q = r[1];
+    const float powMin = r[2].w;
+    CullShape c{};
+    const float t = __fadd_rn(__fmul_rn(-2.08f, powMin), 1e-3f);
+    const float det = __fsub_rn(__fmul_rn(q.x, q.z), __fmul_rn(q.y, q.y));
+    // Infinite box extents: ill-conditioned covariance or no alpha floor.
+    if (!(p.z < __int_as_float(0x7f800000)) || !(det > 0.0f) || !(q.x > 0.0f) || !(q.z > 0.0f))
+        return c;
+    if (!(t > 0.0f)) { // alpha below the floor everywhere
+        c.mode = 1;
+        return c;
+    }
+    c.mode = 2;
+    c.mx = p.x;
+    c.my = p.y;
+    c.B = q.y;
+    c.det = det;
+    c.at = __fmul_rn(q.x, t);
+    c.iA = __frcp_rn(q.x);
+    c.ymax = __fsqrt_rn(__fdiv_rn(__fmul_rn(t, q.x), det));
+    const float xmax = __fsqrt_rn(__fdiv_rn(__fmul_rn(t, q.z), det));
+    c.dyR = __fmul_rn(__fdiv_rn(-q.y, q.z), xmax);
+    return c;
+}
+
+// Tile columns [c0, c1) of tile row ty that the ellipse can reach, within rectangle q.
+__device__ __forceinline__ void cullSpan(const CullShape &c, const int4 &q, int ty, int tileSize, int &c0, int &c1)
+{
+    c0 = q.x;
+    c1 = q.z;
+    if (c.mode == 0)
+        return;
+    const float Y0 = __fsub_rn(float(ty * tileSize), c.my), Y1 = __fadd_rn(Y0, float(tileSize - 1));
+    const float lo = fmaxf(Y0, -c.ymax), hi = fminf(Y1, c.ymax);
+    if (c.mode == 1 || lo > hi) {
+        c1 = c0;
+        return;
+    }
+    const float dyR = fminf(fmaxf(c.dyR, lo), hi), dyL = fminf(fmaxf(-c.dyR, lo), hi);
+    const float sR = __fsqrt_rn(fmaxf(__fsub_rn(c.at, __fmul_rn(c.det, __fmul_rn(dyR, dyR))), 0.0f));
+    const float sL = __fsqrt_rn(fmaxf(__fsub_rn(c.at, __fmul_rn(c.det, __fmul_rn(dyL, dyL))), 0.0f));
+    const float xR = __fmul_rn(__fadd_rn(__fmul_rn(-c.B, dyR), sR), c.iA);
+    const float xL = __fmul_rn(__fsub_rn(__fmul_rn(-c.B, dyL), sL), c.iA);
+    const float inv = 1.0f / float(tileSize); // exact: tile sizes are powers of two
+    const float left = floorf(__fmul_rn(__fsub_rn(__fadd_rn(c.mx, xL), 1.0f), inv));
+    const float right = floorf(__fmul_rn(__fadd_rn(__fadd_rn(c.mx, xR), 1.0f), inv)) + 1.0f;
+    c0 = left > float(q.x) ? int(fminf(left, float(q.z))) : q.x;
+    c1 = right < float(q.z) ? int(fmaxf(right, float(q.x))) : q.z;
+    c1 = max(c1, c0);
+}
+
+__device__ __forceinline__ CullShape shflShape(const CullShape &c, int src)
+{
+    CullShape o;
+    o.mx = __shfl_sync(0xffffffffu, c.mx, src);
+    o.my = __shfl_sync(0xffffffffu, c.my, src);
+    o.B = __shfl_sync(0xffffffffu, c.B, src);
+    o.det = __shfl_sync(0xffffffffu, c.det, src);
+    o.at = __shfl_sync(0xffffffffu, c.at, src);
+    o.iA = __shfl_sync(0xffffffffu, c.iA, src);
+    o.ymax = __shfl_sync(0xffffffffu, c.ymax, src);
+    o.dyR = __shfl_sync(0xffffffffu, c.dyR, src);
+    o.mode = __shfl_sync(0xffffffffu, c.mode, src);
+    return o;
+}
+
+__global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
+                                 int tileSize, int n, int *cnt, int *rankOf)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n)
@@ -291,7 +373,16 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
     int c = 0;
     if (radius[g] > 0) {
         const int4 q = rect[g];
-        c = (q.z - q.x) * (q.w - q.y);
+        if (cullRec == nullptr) {
+            c = (q.z - q.x) * (q.w - q.y);
+        } else {
+            const CullShape cs = cullShape(cullRec, g);
+            for (int ty = q.y; ty < q.w; ++ty) {
+                int c0, c1;
+                cullSpan(cs, q, ty, tileSize, c0, c1);
+                c += c1 - c0;
+            }
+        }
     }
     cnt[r] = c;
 }
@@ -320,7 +411,8 @@ __global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int
 // the next rank, so the search lands on the rank that owns the slot), then its tile in that rank's
 // rectangle (row-major, as the reference's ty/tx loops).
 __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n,
-                                                  const BinCounts *c, int tilesX, uint32_t *keys, int *emitGid)
+                                                  const BinCounts *c, int tilesX, const SplatRec *cullRec, int tileSize,
+                                                  uint32_t *keys, int *emitGid)
 {
     const int total = c->effTotal;
     if (total <= 0)
@@ -333,9 +425,12 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
         const int o = valid ? offs[r] : INT_MAX;
         int g = 0;
         int4 q = make_int4(0, 0, 1, 1);
+        CullShape cs{};
         if (valid) {
             g = int(sortedIds[r]);
             q = rect[g];
+            if (cullRec != nullptr)
+                cs = cullShape(cullRec, g);
         }
         const int first = offs[w * 32], last = min(offs[min(w * 32 + 32, n)], total);
         for (int e0 = first; e0 < last; e0 += 32) {
@@ -350,11 +445,31 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
             const int ol = __shfl_sync(0xffffffffu, o, l);
             const int gl = __shfl_sync(0xffffffffu, g, l);
             const int qx = __shfl_sync(0xffffffffu, q.x, l), qy = __shfl_sync(0xffffffffu, q.y, l);
-            const int qz = __shfl_sync(0xffffffffu, q.z, l);
+            const int qz = __shfl_sync(0xffffffffu, q.z, l), qw = __shfl_sync(0xffffffffu, q.w, l);
+            const CullShape csl = cullRec != nullptr ? shflShape(cs, l) : cs;
             if (e < last) {
-                const int k = e - ol;
-                const int wdt = qz - qx;
-                const int ty = qy + k / wdt, tx = qx + k % wdt;
+                int k = e - ol;
+                int ty, tx;
+                if (cullRec == nullptr) {
+                    const int wdt = qz - qx;
+                    ty = qy + k / wdt;
+                    tx = qx + k % wdt;
+                } else {
+                    // The k-th reachable tile in row-major order: walk the rows' spans.
+                    const int4 qq = make_int4(qx, qy, qz, qw);
+                    ty = qy;
+                    tx = qx;
+                    for (int row = qy; row < qw; ++row) {
+                        int c0, c1;
+                        cullSpan(csl, qq, row, tileSize, c0, c1);
+                        if (k < c1 - c0) {
+                            ty = row;
+                            tx = c0 + k;
+                            break;
+                        }
+                        k -= c1 - c0;
+                    }
+                }
                 keys[e] = uint32_t(ty * tilesX + tx);
                 emitGid[e] = gl;
             }
@@ -442,11 +557,11 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
     { scanDownsweepKernel<<<B, kThreads, 0, s>>>(in, out, n, partial, B); countLaunch(); }
 }
 
-void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, int n, int *cnt, int *rankOf,
-                      cudaStream_t s)
+void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
+                      int tileSize, int n, int *cnt, int *rankOf, cudaStream_t s)
 {
     if (n > 0)
-        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, n, cnt, rankOf); countLaunch(); }
+        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf); countLaunch(); }
 }
 
 namespace {
@@ -465,10 +580,10 @@ void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int itera
 }
 
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
-                int tilesX, uint32_t *keys, int *emitGid, cudaStream_t s)
+                int tilesX, const SplatRec *cullRec, int tileSize, uint32_t *keys, int *emitGid, cudaStream_t s)
 {
     if (n > 0 && capacity > 0)
-        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, keys, emitGid); countLaunch(); }
+        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, cullRec, tileSize, keys, emitGid); countLaunch(); }
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,

@@ -385,6 +385,16 @@ int u3dg_trainer_set_raster_schedule(u3dg_trainer *trainer, int forward_block, i
     });
 }
 
+int u3dg_trainer_set_tile_culling(u3dg_trainer *trainer, int enable)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        t.finish();
+        t.ws.cullTiles = enable != 0;
+        t.stepGraph.reset(); // its emission kernels were recorded with the other setting
+    });
+}
+
 int u3dg_trainer_graph_launches(u3dg_trainer *trainer, long long *launches)
 {
     return guarded([&] {

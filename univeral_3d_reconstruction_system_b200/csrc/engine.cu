@@ -160,10 +160,11 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, &counts.p->n, std::max(n, 1), 32, hist.p,
                    rowTotals.p, &keysOut, &valsOut, stream);
     sortedIds = valsOut;
-    launchRankCounts(sortedIds, rect.p, radius.p, n, cnt.p, rankOf.p, stream);
+    const SplatRec *cullRec = cullTiles ? rec.p : nullptr;
+    launchRankCounts(sortedIds, rect.p, radius.p, cullRec, st.tile_size, n, cnt.p, rankOf.p, stream);
     exclusiveScan(cnt.p, offs.p, n, scanPartial.p, stream);
     launchCapacityCheck(offs.p + n, icap, counts.p, iteration, stream, desc);
-    launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, iKeys0.p, emitGid.p, stream);
+    launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, cullRec, st.tile_size, iKeys0.p, emitGid.p, stream);
     int bits = 0;
     while ((1 << bits) < tiles)
         ++bits;
@@ -298,6 +299,7 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     U3DG_CUDA(cudaGetDevice(&device));
     U3DG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     extent = std::max(sceneExtent, 1e-6f);
+    ws.cullTiles = true;
     n = int(initial.count);
     cap = std::max<size_t>(size_t(std::max(o.max_gaussians, 0)), initial.count);
     cap = std::max<size_t>(cap, 1);

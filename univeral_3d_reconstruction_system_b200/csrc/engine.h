@@ -165,6 +165,9 @@ struct RasterWorkspace {
     // for tiles of 16 and 32 pixels) and the list entries each compositing thread stages per
     // shared-memory batch (1 or 2).
     int forwardBlock = 8, forwardDepth = 1, backwardDepth = 1;
+    // Tile culling: list a Gaussian only in the tiles of its rectangle that its contributing ellipse
+    // can reach (trainers; the rasterizer unit boundary keeps the reference's lists).
+    bool cullTiles = false;
     u3dg_camera cam{};
     u3dg_raster_settings st{};
     uint32_t *sortedIds = nullptr;
