@@ -276,7 +276,7 @@ int u3dg_densify_and_prune(u3dg_model *model, u3dg_model *adam_m, u3dg_model *ad
  * and options[s] (each with its own schedule and Gaussian cap). Every scene keeps its own trainer and
  * stream; u3dg_batch_step advances each scene by `count` iterations (or to its end), interleaving the
  * scenes so their kernels run concurrently and running steps through each scene's step graph where
- * it can. With autotune != 0, each scene's tile size (8, 16 or 32) and compositing schedule (the
+ * it can. With autotune != 0, each scene's tile size (8 or 16) and compositing schedule (the
  * settings of u3dg_trainer_set_raster_schedule; same results for any) are chosen at creation from
  * short timed runs on throwaway trainers; tile_size reports the tile and the tuned ms per step (0
  * without autotune), schedule the compositing settings as well. batch_trainer

@@ -51,7 +51,7 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
         tile, tuned = b.tile_size(k)
         tile2, raster, tuned2 = b.schedule(k)
         assert (tile2, tuned2) == (tile, tuned)
-        assert tile in (8, 16, 32) and raster[0] in (8, 16) and raster[1] in (1, 2) and raster[2] in (1, 2)
+        assert tile in (8, 16) and raster[0] in (8, 16) and raster[1] in (1, 2) and raster[2] in (1, 2)
         if not autotune:
             assert (tile, raster, tuned) == (16, (8, 1, 1), 0.0)
         else:
@@ -59,13 +59,7 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
         t = b.trainer(k)
         assert t.iteration() == 250
         flat, st = _alone(u3dg, scene, tile, raster, 250)
-        got = t.model().flat()
-        if tile == 32:
-            # Tiles of 32 pixels span four CTAs that add their partial gradients atomically: the same
-            # trajectory up to float summation order.
-            assert abs(t.stats().psnr - st.psnr) < 0.1
-        else:
-            np.testing.assert_array_equal(got, flat)
-            s2 = t.stats()
-            assert (s2.iteration, s2.loss, s2.psnr, s2.gaussians) == (st.iteration, st.loss, st.psnr, st.gaussians)
+        np.testing.assert_array_equal(t.model().flat(), flat)
+        s2 = t.stats()
+        assert (s2.iteration, s2.loss, s2.psnr, s2.gaussians) == (st.iteration, st.loss, st.psnr, st.gaussians)
     b.close()

@@ -288,6 +288,8 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
 // Rounding-explicit (the count and the emission kernels get the same spans) and conservative like
 // the compositing kernels' block masks: t widened by 4% + 1e-3 and the span by one pixel each side.
 // Dropping entries that reach no pixel of a tile changes no image and no per-entry gradient.
+constexpr int kCullRows = 8; // rows per rank in the emission's row table
+
 struct CullShape {
     float mx, my, B, det, at, iA, ymax, dyR; // dyR: dy of the rightmost point, (-B / C) xmax
     int mode;                                // 0: whole rectangle, 1: no tile, 2: culled rows
@@ -362,8 +364,11 @@ __device__ __forceinline__ CullShape shflShape(const CullShape &c, int src)
     return o;
 }
 
+// With culling, the first kCullRows rows of every rank's rectangle are also recorded in rowTab[rank *
+// kCullRows + i] as (first column << 16) | (tiles through row i), so the emission finds an entry's row
+// without recomputing spans (rows beyond kCullRows, rare, are recomputed there).
 __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                                 int tileSize, int n, int *cnt, int *rankOf)
+                                 int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n)
@@ -381,6 +386,8 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
                 int c0, c1;
                 cullSpan(cs, q, ty, tileSize, c0, c1);
                 c += c1 - c0;
+                if (ty - q.y < kCullRows)
+                    rowTab[size_t(r) * kCullRows + (ty - q.y)] = (uint32_t(c0) << 16) | uint32_t(c);
             }
         }
     }
@@ -412,7 +419,7 @@ __global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int
 // rectangle (row-major, as the reference's ty/tx loops).
 __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n,
                                                   const BinCounts *c, int tilesX, const SplatRec *cullRec, int tileSize,
-                                                  uint32_t *keys, int *emitGid)
+                                                  const uint32_t *rowTab, uint32_t *keys, int *emitGid)
 {
     const int total = c->effTotal;
     if (total <= 0)
@@ -455,19 +462,37 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
                     ty = qy + k / wdt;
                     tx = qx + k % wdt;
                 } else {
-                    // The k-th reachable tile in row-major order: walk the rows' spans.
-                    const int4 qq = make_int4(qx, qy, qz, qw);
-                    ty = qy;
+                    // The k-th reachable tile in row-major order: the rank's row table, then (rows
+                    // beyond it) the rows' spans.
+                    const uint32_t *tab = rowTab + size_t(w * 32 + l) * kCullRows;
+                    const int rows = qw - qy;
+                    ty = -1;
                     tx = qx;
-                    for (int row = qy; row < qw; ++row) {
-                        int c0, c1;
-                        cullSpan(csl, qq, row, tileSize, c0, c1);
-                        if (k < c1 - c0) {
-                            ty = row;
-                            tx = c0 + k;
+                    int before = 0;
+                    for (int i = 0; i < min(rows, kCullRows); ++i) {
+                        const uint32_t v = tab[i];
+                        const int through = int(v & 0xffffu);
+                        if (k < through) {
+                            ty = qy + i;
+                            tx = int(v >> 16) + (k - before);
                             break;
                         }
-                        k -= c1 - c0;
+                        before = through;
+                    }
+                    if (ty < 0) {
+                        k -= before;
+                        const int4 qq = make_int4(qx, qy, qz, qw);
+                        ty = qy;
+                        for (int row = qy + kCullRows; row < qw; ++row) {
+                            int c0, c1;
+                            cullSpan(csl, qq, row, tileSize, c0, c1);
+                            if (k < c1 - c0) {
+                                ty = row;
+                                tx = c0 + k;
+                                break;
+                            }
+                            k -= c1 - c0;
+                        }
                     }
                 }
                 keys[e] = uint32_t(ty * tilesX + tx);
@@ -557,11 +582,13 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
     { scanDownsweepKernel<<<B, kThreads, 0, s>>>(in, out, n, partial, B); countLaunch(); }
 }
 
+size_t cullRowEntries(size_t n) { return n * kCullRows; }
+
 void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                      int tileSize, int n, int *cnt, int *rankOf, cudaStream_t s)
+                      int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s)
 {
     if (n > 0)
-        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf); countLaunch(); }
+        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf, rowTab); countLaunch(); }
 }
 
 namespace {
@@ -580,10 +607,11 @@ void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int itera
 }
 
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
-                int tilesX, const SplatRec *cullRec, int tileSize, uint32_t *keys, int *emitGid, cudaStream_t s)
+                int tilesX, const SplatRec *cullRec, int tileSize, const uint32_t *rowTab, uint32_t *keys, int *emitGid,
+                cudaStream_t s)
 {
     if (n > 0 && capacity > 0)
-        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, cullRec, tileSize, keys, emitGid); countLaunch(); }
+        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, cullRec, tileSize, rowTab, keys, emitGid); countLaunch(); }
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,

@@ -143,6 +143,7 @@ struct RasterWorkspace {
     DevBuf<float> depth;
     DevBuf<int4> rect;
     DevBuf<int> radius, rankOf, cnt, offs, scanPartial, hist, rowTotals;
+    DevBuf<uint32_t> rowTab; // tile culling: per rank, the first rows' spans (emission lookup)
     DevBuf<uint8_t> flags;
     DevBuf<float4> cov2d;
     DevBuf<float> g2d; // per Gaussian: summed 2D gradients (chain-rule input)
@@ -417,10 +418,10 @@ struct BatchGraph {
 // graph holding all of their chunks (bg, may be null: no combined graph).
 void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph *bg = nullptr);
 
-// Tile size (8, 16 or 32), forward pixel block (8 or 16) and compositing batch depths (1 or 2 staged
-// list entries per thread per batch, for the forward and the backward kernel) with the shortest step
-// time for a scene, timed on throwaway trainers started from the same model. Tile 32, whose partial
-// gradients are added atomically, must be at least 3% faster than the best of 8 and 16.
+// Tile size (8 or 16: the sizes whose results are deterministic), forward pixel block (8 or 16) and
+// compositing batch depths (1 or 2 staged list entries per thread per batch, for the forward and the
+// backward kernel) with the shortest step time for a scene, timed on throwaway trainers started from
+// the same model.
 struct RasterSchedule {
     int tileSize, forwardBlock, forwardDepth, backwardDepth;
     float msPerStep;

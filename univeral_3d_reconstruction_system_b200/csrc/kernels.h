@@ -100,9 +100,11 @@ int radixDigits();
 size_t scanPartialEntries(int n);
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
 // Per depth rank: tile count of the Gaussian and the inverse map gid -> rank. With cullRec (the
-// projected records), only the tiles of the rectangle that the contributing ellipse can reach count.
+// projected records), only the tiles of the rectangle that the contributing ellipse can reach count,
+// and rowTab (cullRowEntries(n) entries) receives the rows' spans for the emission.
+size_t cullRowEntries(size_t n);
 void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                      int tileSize, int n, int *cnt, int *rankOf, cudaStream_t s);
+                      int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s);
 // Sets counts->n and checks *total against the intersection capacity (see BinCounts).
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
                          const StepDesc *desc = nullptr);
@@ -110,7 +112,8 @@ void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 // Emission of the intersections in depth-rank order: tile key and Gaussian id per intersection (the
 // same tiles as launchRankCounts counted).
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
-                int tilesX, const SplatRec *cullRec, int tileSize, uint32_t *keys, int *emitGid, cudaStream_t s);
+                int tilesX, const SplatRec *cullRec, int tileSize, const uint32_t *rowTab, uint32_t *keys, int *emitGid,
+                cudaStream_t s);
 // After the tile sort: Gaussian id per sorted entry and the tile offsets.
 // digitTotals (may be null): the digit totals of a single-pass tile sort, whose exclusive scan gives the
 // tile offsets directly; otherwise they come from a binary search in the sorted keys.
