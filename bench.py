@@ -303,8 +303,10 @@ def run_ours(args, dist: Dist) -> dict:
             "traffic": profiled_traffic(dominant_kernel),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
             # The compositing kernels move few bytes per instruction: their limiter is instruction
-            # issue (FP32 / integer pipes), which the same capture reports.
+            # issue (FP32 / integer pipes), which the same capture reports (percent of peak).
             "issue_active_pct": profiled_metric(dominant_kernel, "smsp__issue_active.avg.pct_of_peak_sustained_active"),
+            "fp32_pipe_pct": profiled_metric(dominant_kernel, "sm__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active"),
+            "alu_pipe_pct": profiled_metric(dominant_kernel, "sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active"),
             "dram_throughput_pct": profiled_metric(dominant_kernel,
                                                    "gpu__dram_throughput.avg.pct_of_peak_sustained_elapsed"),
             "algorithmic_bytes_per_launch": bytes_[dominant],
