@@ -114,9 +114,10 @@ def test_tile_lists_edge_cases(u3dg, oracle):
                 np.zeros((n, 4), np.int32), 3, 2)
     rect1 = np.tile(np.array([0, 0, 1, 1], np.int32), (n, 1))
     _check_bins(u3dg, oracle, rng.uniform(1, 5, n).astype(np.float32), np.ones(n, np.int32), rect1, 1, 1)
-    # Many exact depth ties (ties keep index order), random rectangles, > 256 tiles (two sort passes),
+    # Many exact depth ties (ties keep index order), random rectangles, up to 2048 tiles (one sort pass
+    # that also writes the lists and offsets), more than 2048 (two passes and a separate finalisation),
     # and more items than one sort block.
-    for n, tx, ty, levels in ((5000, 40, 30, 7), (70000, 17, 19, 1000), (3000, 300, 2, 3)):
+    for n, tx, ty, levels in ((5000, 40, 30, 7), (70000, 17, 19, 1000), (3000, 300, 2, 3), (8000, 80, 60, 50)):
         depth = rng.integers(1, levels + 1, n).astype(np.float32) * np.float32(0.5)
         x0 = rng.integers(0, tx, n)
         y0 = rng.integers(0, ty, n)

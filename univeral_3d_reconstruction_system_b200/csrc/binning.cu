@@ -16,7 +16,8 @@
 // replays the step).
 //
 // Sorting: stable LSD passes, 8-bit digits for the depth keys and one 11-bit pass for tile ids (up to
-// 2048 tiles; the tile offsets are then the exclusive scan of that pass's digit totals). A pass is
+// 2048 tiles; that pass's scatter also writes the tile lists' Gaussian ids and, in block 0, the tile
+// offsets, which are the exclusive scan of its digit totals). A pass is
 // three kernels: per-block digit histograms, a per-digit scan over the blocks, and a scatter whose
 // in-block ranks come from warp match-any votes. Every block owns one contiguous chunk of the items
 // and walks it in rounds of kTile items.
@@ -125,10 +126,14 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G,
 // memory; an item's position is its digit's base + the counts of the warps before it (they hold
 // earlier items) + its rank in its warp. After the round the last item of each (warp, digit) advances
 // the digit's base and clears that count, so only the touched counts are reset.
-template <int DB>
+// kTiles (the single pass of a tile sort, digit = tile): instead of the sorted keys, the scatter
+// writes each entry's Gaussian id (fin.list[pos] = fin.emitGid[emission index]), and block 0 writes
+// the tile offsets, which are the digit bases it starts from.
+template <int DB, bool kTiles = false>
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
                                                                uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
-                                                               int shift, const int *hist, const int *rowTotals, int G)
+                                                               int shift, const int *hist, const int *rowTotals, int G,
+                                                               TileFinish fin)
 {
     constexpr int R = 1 << DB;
     __shared__ uint8_t warpCounts[kWarps][R];
@@ -150,6 +155,12 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
         }
     }
     __syncthreads();
+    if (kTiles && blockIdx.x == 0) {
+        for (int d = threadIdx.x; d < fin.tiles; d += kThreads)
+            fin.tileOffsets[d] = base[d]; // block 0's row prefix is zero
+        if (threadIdx.x == 0)
+            fin.tileOffsets[fin.tiles] = *nPtr;
+    }
     const uint32_t lanesBelow = (1u << lane) - 1u;
     uint8_t *myCounts = warpCounts[warp];
     for (int r0 = begin; r0 < end; r0 += kTile) {
@@ -187,7 +198,11 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
                 for (int w = 0; w < warp; ++w)
                     cross += warpCounts[w][d];
                 const int pos = base[d] + cross + local[r];
-                keysOut[pos] = key[r];
+                if (kTiles) {
+                    fin.list[pos] = fin.emitGid[val[r]];
+                } else {
+                    keysOut[pos] = key[r];
+                }
                 valsOut[pos] = val[r];
                 last[r] = local[r] == int(myCounts[d]) - 1;
             }
@@ -204,23 +219,6 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
                 myCounts[digit[r]] = 0;
         __syncthreads();
     }
-}
-
-// Tile offsets of a single-pass tile sort: the exclusive scan of its digit totals (digit = tile).
-__global__ void __launch_bounds__(kThreads) digitOffsetsKernel(const int *rowTotals, int tiles, const BinCounts *c,
-                                                               int *tileOffsets)
-{
-    int carry = 0;
-    for (int c0 = 0; c0 < tiles; c0 += kThreads) {
-        const int t = c0 + threadIdx.x;
-        int total;
-        const int ex = blockExclusiveScan(t < tiles ? rowTotals[t] : 0, total);
-        if (t < tiles)
-            tileOffsets[t] = carry + ex;
-        carry += total;
-    }
-    if (threadIdx.x == 0)
-        tileOffsets[tiles] = c->effTotal;
 }
 
 // Exclusive scan, reduce-then-scan over a host-known n.
@@ -537,7 +535,8 @@ size_t radixHistEntries(int nMax) { return size_t(1 << kWideBits) * size_t(radix
 int radixDigits() { return 1 << kWideBits; }
 
 int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
-                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s)
+                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
+                   const TileFinish *fin)
 {
     uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
     const uint32_t *vin = nullptr;
@@ -545,17 +544,22 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     // Keys of up to 11 bits (tile ids) in one pass of 2048 digits; longer keys in 8-bit passes (three
     // 11-bit passes over 32-bit depth keys measured slower than four 8-bit ones).
     const bool wide = bits <= kWideBits;
+    if (!wide)
+        fin = nullptr;
     const int db = wide ? kWideBits : 8;
     int passes = 0;
     for (int shift = 0; shift < bits; shift += db, ++passes) {
         if (wide) {
             { radixHistKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
             { radixRowScanKernel<<<1 << kWideBits, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
-            { radixScatterKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+            if (fin != nullptr)
+                { radixScatterKernel<kWideBits, true><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, *fin); countLaunch(); }
+            else
+                { radixScatterKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         } else {
             { radixHistKernel<8><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
             { radixRowScanKernel<<<1 << 8, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
-            { radixScatterKernel<8><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G); countLaunch(); }
+            { radixScatterKernel<8><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         }
         uint32_t *nk = kin;
         kin = kout;
@@ -615,14 +619,11 @@ void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, in
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, const int *digitTotals, cudaStream_t s)
+                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s)
 {
     if (capacity > 0)
         { finalizeKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedEmit, emitGid, c, list); countLaunch(); }
-    if (digitTotals != nullptr && tiles <= (1 << kWideBits))
-        { digitOffsetsKernel<<<1, kThreads, 0, s>>>(digitTotals, tiles, c, tileOffsets); countLaunch(); }
-    else
-        { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
+    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
 }
 
 } // namespace u3dg

@@ -172,11 +172,13 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     while ((1 << bits) < tiles)
         ++bits;
     bits = std::max(bits, 1);
-    const int tilePasses = radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits, hist.p, rowTotals.p,
-                   &keysOut, &valsOut, stream);
+    // Up to 2048 tiles: one pass whose scatter also writes the lists' Gaussian ids and the tile offsets.
+    const TileFinish fin{emitGid.p, list.p, tileOffsets.p, tiles};
+    const int tilePasses = radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits,
+                                          hist.p, rowTotals.p, &keysOut, &valsOut, stream, &fin);
     listEmit = valsOut;
-    launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p,
-                       tilePasses == 1 ? rowTotals.p : nullptr, stream);
+    if (tilePasses != 1)
+        launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p, stream);
 }
 
 void RasterWorkspace::forwardChecked(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,

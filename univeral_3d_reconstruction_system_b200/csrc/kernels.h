@@ -88,13 +88,23 @@ void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float ca
 // Blocks of a radix pass sized for at most nMax items, and the histogram entries it needs.
 int radixBlocks(int nMax);
 size_t radixHistEntries(int nMax);
+// Outputs of a tile sort done in one pass (keys of at most 11 bits, digit = tile): the scatter writes
+// the Gaussian id of every sorted entry (list[pos] = emitGid[emission index]) instead of the sorted
+// keys, and the tile offsets (tiles + 1 entries; the last is the item count).
+struct TileFinish {
+    const int *emitGid;
+    int *list;
+    int *tileOffsets;
+    int tiles;
+};
 // Stable LSD radix sort of (key, value) pairs on key bits [0, bits); the item count is read on the
 // device from *nDev (at most nMax); the initial values are the item indices. Result in *keysOut /
 // *valsOut (one of the two buffers).
-// Returns the number of passes (11-bit digits); rowTotals needs radixDigits() entries and holds the
-// digit totals of the last pass.
+// Returns the number of passes; rowTotals needs radixDigits() entries. fin (may be null) applies when
+// bits <= 11 (one pass): *keysOut is then not written.
 int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
-                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s);
+                   int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
+                   const TileFinish *fin = nullptr);
 int radixDigits();
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
@@ -114,11 +124,10 @@ void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
                 int tilesX, const SplatRec *cullRec, int tileSize, const uint32_t *rowTab, uint32_t *keys, int *emitGid,
                 cudaStream_t s);
-// After the tile sort: Gaussian id per sorted entry and the tile offsets.
-// digitTotals (may be null): the digit totals of a single-pass tile sort, whose exclusive scan gives the
-// tile offsets directly; otherwise they come from a binary search in the sorted keys.
+// After a tile sort of several passes (more than 2048 tiles): Gaussian id per sorted entry and the tile
+// offsets (a binary search in the sorted keys). A one-pass tile sort writes both itself (TileFinish).
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, const int *digitTotals, cudaStream_t s);
+                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s);
 
 // raster.cu
 struct RasterArgs {
