@@ -340,7 +340,9 @@ void u3dg_adam_destroy(u3dg_adam *adam);
 /* ------------------------------------------------------------------ model I/O and init (host) */
 
 /* initGaussiansFromPoints (engine/include/u3d/splat/GaussianModel.h:41,
- * engine/src/splat/GaussianModel.cpp:68-144): xyz 3n, rgb 3n (0..1, NULL = grey); out arrays n. */
+ * engine/src/splat/GaussianModel.cpp:68-144): xyz 3n, rgb 3n (0..1, NULL = grey); out arrays n (host
+ * memory). The hash grid is built on the host and the 27-cell nearest-neighbour search runs on the
+ * current GPU; the result is bit-identical to the reference's. Needs a GPU (U3DG_ERR_NO_DEVICE). */
 int u3dg_init_gaussians_from_points(const float *xyz, const float *rgb, size_t n, u3dg_model *out);
 /* writeSplatPly (engine/include/u3d/splat/SplatPly.h:12, engine/src/splat/SplatPly.cpp:261-282). */
 int u3dg_write_splat_ply(const char *path, const u3dg_model *model);

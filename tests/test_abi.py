@@ -1,5 +1,6 @@
 """The C ABI library without a GPU: it loads, exports every entry point include/u3dg.h declares,
-its host-only entry points (defaults, initGaussiansFromPoints, PLY I/O) match the reference, and
+its host-only entry points (defaults, PLY I/O with the host-side initGaussiansFromPoints for point
+clouds) match the reference, and
 entry points that need a GPU fail with a status code instead of crashing when there is none."""
 import ctypes as C
 import re
@@ -54,20 +55,6 @@ def test_option_defaults_match_reference(reference):
             assert TrainOptions.for_iterations(it).struct_tuple() == TrainOptions.from_struct(o).struct_tuple()
 
 
-@pytest.mark.parametrize("n", [0, 1, 2, 4, 1000, 20000])
-def test_init_from_points_matches_reference(reference, n):
-    rng = np.random.default_rng(n)
-    # Clustered points exercise hash-grid buckets with many members and repeated keys.
-    xyz = (rng.normal(size=(n, 3)) * rng.choice([0.01, 1.0], size=(n, 1))).astype(np.float32)
-    rgb = rng.uniform(size=(n, 3)).astype(np.float32)
-    a = api.initGaussiansFromPoints(xyz, rgb)
-    b = reference.init_from_points(xyz, rgb)
-    for name in GROUPS_ORDER:
-        np.testing.assert_array_equal(getattr(a, name), getattr(b, name))
-    g = api.initGaussiansFromPoints(xyz)  # no colours: grey
-    np.testing.assert_array_equal(g.colors, reference.init_from_points(xyz).colors)
-
-
 def test_ply_round_trip_and_reference_compatibility(reference, tmp_path):
     """ply_round_trip (test_splat.cpp:270-298): our writer / reader against the reference's."""
     rng = np.random.default_rng(5)
@@ -82,22 +69,28 @@ def test_ply_round_trip_and_reference_compatibility(reference, tmp_path):
     assert is_splat and r.size() == n
     for name in GROUPS_ORDER:
         np.testing.assert_array_equal(getattr(r, name), getattr(m, name))
-    # A plain point cloud becomes opaque Gaussians (SplatPly.cpp:301-321); compare with the reference.
-    pts = tmp_path / "points.ply"
-    xyz = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
-    lines = ["ply", "format ascii 1.0", "element vertex 4", "property float x", "property float y",
-             "property float z", "property uchar red", "property uchar green", "property uchar blue", "end_header"]
-    cols = [(255, 0, 0), (0, 255, 0), (0, 0, 255), (255, 255, 255)]
-    lines += [f"{x} {y} {z} {r_} {g_} {b_}" for (x, y, z), (r_, g_, b_) in zip(xyz, cols)]
-    pts.write_text("\n".join(lines) + "\n")
-    r, is_splat = api.readSplatPly(str(pts))
-    assert not is_splat and r.size() == 4
-    cnt, flag = C.c_size_t(), C.c_int()
-    out = GaussianModel.zeros(4)
-    ov = out.view()
-    assert reference.lib.ref_read_splat_ply(str(pts).encode(), C.byref(ov), C.byref(cnt), C.byref(flag)) == 1
-    for name in GROUPS_ORDER:
-        np.testing.assert_array_equal(getattr(r, name), getattr(out, name))
+    # A plain point cloud becomes opaque Gaussians (SplatPly.cpp:301-321) through the host-side
+    # initGaussiansFromPoints (hash-grid 3-NN); compare with the reference, on 4 points and on a
+    # clustered cloud whose hash-grid buckets have many members and repeated keys.
+    rng2 = np.random.default_rng(9)
+    clustered = (rng2.normal(size=(3000, 3)) * rng2.choice([0.01, 1.0], size=(3000, 1))).astype(np.float32)
+    for k, xyz in enumerate((np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32), clustered)):
+        pts = tmp_path / f"points{k}.ply"
+        cols = rng2.integers(0, 256, (len(xyz), 3))
+        lines = ["ply", "format ascii 1.0", f"element vertex {len(xyz)}", "property float x", "property float y",
+                 "property float z", "property uchar red", "property uchar green", "property uchar blue",
+                 "end_header"]
+        lines += [f"{x!r} {y!r} {z!r} {r_} {g_} {b_}" for (x, y, z), (r_, g_, b_) in
+                  zip(xyz.tolist(), cols.tolist())]
+        pts.write_text("\n".join(lines) + "\n")
+        r, is_splat = api.readSplatPly(str(pts))
+        assert not is_splat and r.size() == len(xyz)
+        cnt, flag = C.c_size_t(), C.c_int()
+        out = GaussianModel.zeros(len(xyz))
+        ov = out.view()
+        assert reference.lib.ref_read_splat_ply(str(pts).encode(), C.byref(ov), C.byref(cnt), C.byref(flag)) == 1
+        for name in GROUPS_ORDER:
+            np.testing.assert_array_equal(getattr(r, name), getattr(out, name))
     res = api.PlyResult()
     assert api.readSplatPly(str(tmp_path / "missing.ply"), res) == (None, False)
     assert "Cannot open" in res.error
@@ -114,6 +107,9 @@ def test_gpu_entry_points_fail_cleanly_without_a_device():
         api.Trainer(m, [], 1.0, TrainOptions())
     with pytest.raises(api.U3dgError):
         api.psnr(np.zeros(3, np.float32), np.zeros(3, np.float32))
+    with pytest.raises(api.U3dgError) as e:
+        api.initGaussiansFromPoints(np.zeros((4, 3), np.float32))
+    assert e.value.status == _abi.ERR_NO_DEVICE
 
 
 def test_invalid_arguments_are_rejected():

@@ -33,6 +33,25 @@ def _views(sc, k=4):
     return sc.cameras[:k]
 
 
+# ------------------------------------------------------------------ initialisation
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 4, 1000, 20000, 200000])
+def test_init_from_points_matches_reference(u3dg, reference, n):
+    """initGaussiansFromPoints with its hash-grid 3-NN search on the GPU is bit-identical to the
+    reference's host version (clustered points: buckets with many members and repeated keys)."""
+    rng = np.random.default_rng(n)
+    xyz = (rng.normal(size=(n, 3)) * rng.choice([0.01, 1.0], size=(n, 1))).astype(np.float32)
+    rgb = rng.uniform(size=(n, 3)).astype(np.float32)
+    a = u3dg.initGaussiansFromPoints(xyz, rgb)
+    b = reference.init_from_points(xyz, rgb)
+    for name in GROUPS:
+        np.testing.assert_array_equal(getattr(a, name), getattr(b, name))
+    if n <= 20000:
+        g = u3dg.initGaussiansFromPoints(xyz)  # no colours: grey
+        np.testing.assert_array_equal(g.colors, reference.init_from_points(xyz).colors)
+
+
 # ------------------------------------------------------------------ projection
 
 

@@ -411,6 +411,8 @@ def densifyAndPrune(model: GaussianModel, m: GaussianModel, v: GaussianModel, gr
 
 
 def initGaussiansFromPoints(xyz: np.ndarray, rgb: np.ndarray | None = None) -> GaussianModel:
+    """initGaussiansFromPoints (GaussianModel.cpp:68-144): hash-grid 3-NN scales, identity rotations,
+    opacity 0.1, colours from rgb (grey without). The neighbour search runs on the GPU."""
     x = np.ascontiguousarray(xyz, np.float32).reshape(-1)
     n = x.size // 3
     out = GaussianModel.zeros(n)

@@ -1003,7 +1003,8 @@ int u3dg_init_gaussians_from_points(const float *xyz, const float *rgb, size_t n
             throw StatusError(U3DG_ERR_INVALID_ARG, "NULL argument");
         if (n)
             requireModel(out, "out");
-        initGaussiansFromPointsHost(xyz, rgb, n, *out);
+        requireDevice();
+        initGaussiansFromPointsDevice(xyz, rgb, n, *out);
     });
 }
 

@@ -3,6 +3,7 @@
 
 #include "../../include/u3dg.h"
 
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -21,8 +22,25 @@ struct HostModel {
     }
 };
 
-// initGaussiansFromPoints (GaussianModel.cpp:68-144); out must hold n Gaussians.
+// initGaussiansFromPoints (GaussianModel.cpp:68-144) on the host; out must hold n Gaussians. Used by
+// the PLY reader for point clouds (readSplatPly does the same in the reference).
 void initGaussiansFromPointsHost(const float *xyz, const float *rgb, size_t n, u3dg_model &out);
+
+// Its pieces, shared with the GPU version (initGaussiansFromPointsDevice): the hash grid
+// (GaussianModel.cpp:72-98), the cell key, and the model written from every point's 3 smallest
+// squared neighbour distances (best[3n], FLT_MAX where fewer were found; GaussianModel.cpp:122-142).
+struct InitGrid {
+    float cell = 0.0f;
+    std::vector<int> cx, cy, cz;  // cell coordinates per point
+    std::vector<int64_t> keys;    // cell keys, sorted
+    std::vector<uint32_t> ids;    // point index per sorted key (ties in index order)
+};
+int64_t initHashKey(int x, int y, int z);
+void buildInitGrid(const float *xyz, size_t n, InitGrid &g);
+void finishInitFromNeighbours(const float *xyz, const float *rgb, size_t n, float cell, const float *best,
+                              u3dg_model &out);
+// The same initialisation with the 27-cell neighbour search on the current GPU (bit-identical).
+void initGaussiansFromPointsDevice(const float *xyz, const float *rgb, size_t n, u3dg_model &out);
 // writeSplatPly (SplatPly.cpp:261-282).
 bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error);
 // readSplatPly (SplatPly.cpp:284-342).

@@ -224,7 +224,7 @@ void plainInit(const float *xyz, const float *rgb, size_t n, HostModel &base, st
 {
     base.resize(n);
     u3dg_model v{base.means.data(), base.scales.data(), base.quats.data(), base.opac.data(), base.colors.data(), n};
-    initGaussiansFromPointsHost(xyz, rgb, n, v);
+    initGaussiansFromPointsDevice(xyz, rgb, n, v);
     sigma.resize(n);
     for (size_t i = 0; i < n; ++i)
         sigma[i] = std::exp(base.scales[3 * i]);
