@@ -61,6 +61,8 @@ class Dist:
 
             import torch
             import torch.distributed as dist
+            if backend is None and not torch.cuda.is_available():
+                self.backend = "gloo"  # no GPU: the reference arm's ranks on the host cores
             if self.backend == "nccl":
                 torch.cuda.set_device(self.local)
                 dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
@@ -495,8 +497,9 @@ def run_reference(args, dist: Dist) -> dict | None:
             "warmup": W, "ms_per_step": dt * 1e3 / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config(args, dist),
             "cpu_baseline": {"value": v, "unit": "it/s", "kind": "reference", "cores": threads,
-                             "sample": f"{K} steps after {W} warm-up steps of the high-300k workload "
-                                       f"(requested {args.steps} / {args.warmup}; capped to bound the CPU time)"},
+                             "sample": f"{K} steps after {W} warm-up steps of the {args.workload} workload "
+                                       f"(requested {args.steps} / {args.warmup}; at most 60 / 3 to bound the CPU "
+                                       f"time)"},
             "e2e": {"value": v, "unit": "it/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
