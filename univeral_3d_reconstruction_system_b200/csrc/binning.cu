@@ -286,7 +286,8 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
 // Rounding-explicit (the count and the emission kernels get the same spans) and conservative like
 // the compositing kernels' block masks: t widened by 4% + 1e-3 and the span by one pixel each side.
 // Dropping entries that reach no pixel of a tile changes no image and no per-entry gradient.
-constexpr int kCullRows = 8; // rows per rank in the emission's row table
+constexpr int kCullRows = 8; // rows per rank in the emission's row table (32 bytes: two uint4 loads)
+static_assert(kCullRows == 8, "the emission reads a rank's row table as two uint4");
 
 struct CullShape {
     float mx, my, B, det, at, iA, ymax, dyR; // dyR: dy of the rightmost point, (-B / C) xmax
@@ -345,21 +346,6 @@ __device__ __forceinline__ void cullSpan(const CullShape &c, const int4 &q, int 
     c0 = left > float(q.x) ? int(fminf(left, float(q.z))) : q.x;
     c1 = right < float(q.z) ? int(fmaxf(right, float(q.x))) : q.z;
     c1 = max(c1, c0);
-}
-
-__device__ __forceinline__ CullShape shflShape(const CullShape &c, int src)
-{
-    CullShape o;
-    o.mx = __shfl_sync(0xffffffffu, c.mx, src);
-    o.my = __shfl_sync(0xffffffffu, c.my, src);
-    o.B = __shfl_sync(0xffffffffu, c.B, src);
-    o.det = __shfl_sync(0xffffffffu, c.det, src);
-    o.at = __shfl_sync(0xffffffffu, c.at, src);
-    o.iA = __shfl_sync(0xffffffffu, c.iA, src);
-    o.ymax = __shfl_sync(0xffffffffu, c.ymax, src);
-    o.dyR = __shfl_sync(0xffffffffu, c.dyR, src);
-    o.mode = __shfl_sync(0xffffffffu, c.mode, src);
-    return o;
 }
 
 // With culling, the first kCullRows rows of every rank's rectangle are also recorded in rowTab[rank *
@@ -430,12 +416,9 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
         const int o = valid ? offs[r] : INT_MAX;
         int g = 0;
         int4 q = make_int4(0, 0, 1, 1);
-        CullShape cs{};
         if (valid) {
             g = int(sortedIds[r]);
             q = rect[g];
-            if (cullRec != nullptr)
-                cs = cullShape(cullRec, g);
         }
         const int first = offs[w * 32], last = min(offs[min(w * 32 + 32, n)], total);
         for (int e0 = first; e0 < last; e0 += 32) {
@@ -451,7 +434,6 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
             const int gl = __shfl_sync(0xffffffffu, g, l);
             const int qx = __shfl_sync(0xffffffffu, q.x, l), qy = __shfl_sync(0xffffffffu, q.y, l);
             const int qz = __shfl_sync(0xffffffffu, q.z, l), qw = __shfl_sync(0xffffffffu, q.w, l);
-            const CullShape csl = cullRec != nullptr ? shflShape(cs, l) : cs;
             if (e < last) {
                 int k = e - ol;
                 int ty, tx;
@@ -462,13 +444,19 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
                 } else {
                     // The k-th reachable tile in row-major order: the rank's row table, then (rows
                     // beyond it) the rows' spans.
-                    const uint32_t *tab = rowTab + size_t(w * 32 + l) * kCullRows;
+                    // One 32-byte row (two vector loads) per rank; entries past its rows are unused.
+                    const uint4 *tab = reinterpret_cast<const uint4 *>(rowTab + size_t(w * 32 + l) * kCullRows);
+                    const uint4 t0 = tab[0], t1 = tab[1];
+                    const uint32_t tv[kCullRows] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
                     const int rows = qw - qy;
                     ty = -1;
                     tx = qx;
                     int before = 0;
-                    for (int i = 0; i < min(rows, kCullRows); ++i) {
-                        const uint32_t v = tab[i];
+#pragma unroll
+                    for (int i = 0; i < kCullRows; ++i) {
+                        if (i >= rows)
+                            break;
+                        const uint32_t v = tv[i];
                         const int through = int(v & 0xffffu);
                         if (k < through) {
                             ty = qy + i;
@@ -477,8 +465,9 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
                         }
                         before = through;
                     }
-                    if (ty < 0) {
+                    if (ty < 0) { // rare: more rows than the table holds
                         k -= before;
+                        const CullShape csl = cullShape(cullRec, gl);
                         const int4 qq = make_int4(qx, qy, qz, qw);
                         ty = qy;
                         for (int row = qy + kCullRows; row < qw; ++row) {
