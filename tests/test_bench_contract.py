@@ -53,3 +53,19 @@ def test_reference_arm_under_torchrun_two_ranks(reference_built):
     lines = _lines(r.stdout)
     assert len(lines) == 1
     _check(lines[0], 2)
+
+
+def test_roofline_figures_come_from_the_committed_profiles():
+    """The bench's roofline line reads the dominant kernels' DRAM traffic and pipe utilisation from the
+    committed ncu summaries (profiles/*_high-300k.md)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    for kernel in ("compositeBackwardKernel", "compositeForwardKernel", "chainKernel"):
+        traffic = bench.profiled_traffic(kernel)
+        assert traffic is not None and traffic > 1e6, kernel
+        for metric in ("smsp__issue_active.avg.pct_of_peak_sustained_active",
+                       "sm__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active",
+                       "gpu__dram_throughput.avg.pct_of_peak_sustained_elapsed"):
+            v = bench.profiled_metric(kernel, metric)
+            assert v is not None and 0.0 <= v <= 100.0, (kernel, metric, v)
+    assert bench.profiled_traffic("noSuchKernel") is None
