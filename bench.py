@@ -327,6 +327,11 @@ def run_ours(args, dist: Dist) -> dict:
     res["workload_stats"].update({
         "gaussians_pixels_per_s": n * p * it_s,
         "pair_evaluations_per_s": i_avg * 256 * it_s,  # E = sum over tiles of pixels x list length (16x16)
+        # Nominal FP32 work of the compositing passes (reported, not graded): about 12 FLOP + 1 exp per
+        # forward and 35 FLOP + 1 exp per backward pair evaluation, over E pairs per pass (an upper
+        # bound: the per-warp culling skips many of them).
+        "compositing_flops_per_s_nominal": i_avg * 256 * (12 + 35) * it_s,
+        "compositing_exps_per_s_nominal": i_avg * 256 * 2 * it_s,
     })
     if args.schedule:
         res["schedule"] = run_full_schedule(args, sc)
