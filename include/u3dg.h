@@ -180,6 +180,10 @@ int u3dg_trainer_size(u3dg_trainer *trainer, size_t *count);
 /* Trainer::model (Trainer.h:55): copies the current model into host arrays of capacity `capacity`
  * Gaussians (U3DG_ERR_CAPACITY if too small; *count is set either way). */
 int u3dg_trainer_download(u3dg_trainer *trainer, u3dg_model *out, size_t capacity, size_t *count);
+/* writeSplatPly(path, trainer.model()) (Reconstructor.cpp:350-355, SplatPly.cpp:261-282) in one call:
+ * the trainer's current model is copied from the GPU into a temporary host copy and written; the same
+ * bytes as u3dg_trainer_download followed by u3dg_write_splat_ply. */
+int u3dg_trainer_write_splat_ply(u3dg_trainer *trainer, const char *path);
 /* Trainer::evaluatePsnr (Trainer.cpp:180-192): mean PSNR over all training views. */
 int u3dg_trainer_eval_psnr(u3dg_trainer *trainer, float *psnr);
 /* Trainer::render (Trainer.cpp:194-197): rgb gets height*width*3 floats. */

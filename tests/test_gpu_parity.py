@@ -551,6 +551,24 @@ def test_forward_on_8x8_blocks_is_bit_exact(u3dg, tiny_scene, tile, depth):
         np.testing.assert_array_equal(out[0], out[1])
 
 
+def test_trainer_writes_the_reference_ply(u3dg, oracle, reference, tiny_scene, tmp_path):
+    """The trainer's one-call PLY export writes the same bytes as downloading the model and writing it
+    with this library's writer or with the reference's (SplatPly.cpp:261-282)."""
+    import ctypes as C
+    sc = tiny_scene
+    t = u3dg.Trainer(oracle.init_from_points(sc.init_xyz, sc.init_rgb), sc.images, sc.extent, sc.options())
+    t.step(120)
+    direct, via, ref = tmp_path / "direct.ply", tmp_path / "via.ply", tmp_path / "ref.ply"
+    t.writeSplatPly(str(direct))
+    m = t.model()
+    assert u3dg.writeSplatPly(str(via), m)
+    v = m.view()
+    assert reference.lib.ref_write_splat_ply(str(ref).encode(), C.byref(v)) == 1
+    assert direct.read_bytes() == via.read_bytes() == ref.read_bytes()
+    with pytest.raises(u3dg.U3dgError):
+        t.writeSplatPly(str(tmp_path / "no_such_dir" / "x.ply"))
+
+
 def test_training_recovers_a_synthetic_scene(u3dg, oracle):
     """training_recovers_a_synthetic_scene (test_splat.cpp:227-268) on the GPU."""
     rng = np.random.default_rng(11)

@@ -50,6 +50,7 @@ SIGNATURES = {
     "u3dg_trainer_size": (C.c_int, [_P, _SZ]),
     "u3dg_trainer_download": (C.c_int, [_P, _MV, C.c_size_t, _SZ]),
     "u3dg_trainer_eval_psnr": (C.c_int, [_P, _F]),
+    "u3dg_trainer_write_splat_ply": (C.c_int, [_P, C.c_char_p]),
     "u3dg_trainer_render": (C.c_int, [_P, _CAM, _F]),
     "u3dg_trainer_stream": (C.c_int, [_P, _PP]),
     "u3dg_trainer_synchronize": (C.c_int, [_P]),

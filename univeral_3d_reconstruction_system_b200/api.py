@@ -96,6 +96,10 @@ class Trainer:
         check(load().u3dg_trainer_eval_psnr(self._h, C.byref(p)))
         return float(p.value)
 
+    def writeSplatPly(self, path: str) -> None:
+        """writeSplatPly(path, model()) in one call (u3dg_trainer_write_splat_ply)."""
+        check(load().u3dg_trainer_write_splat_ply(self._h, str(path).encode()))
+
     evaluate_psnr = evaluatePsnr
 
     def render(self, camera: RenderCamera) -> np.ndarray:

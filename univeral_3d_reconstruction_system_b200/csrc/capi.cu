@@ -272,6 +272,23 @@ int u3dg_trainer_download(u3dg_trainer *trainer, u3dg_model *out, size_t capacit
     });
 }
 
+int u3dg_trainer_write_splat_ply(u3dg_trainer *trainer, const char *path)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        if (!path)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "path is NULL");
+        t.finish();
+        HostModel m;
+        m.resize(size_t(t.n));
+        u3dg_model v{m.means.data(), m.scales.data(), m.quats.data(), m.opac.data(), m.colors.data(), m.size()};
+        t.download(v);
+        std::string err;
+        if (!writeSplatPlyHost(path, v, &err))
+            throw StatusError(U3DG_ERR_IO, err);
+    });
+}
+
 int u3dg_trainer_eval_psnr(u3dg_trainer *trainer, float *psnr)
 {
     return guarded([&] {
