@@ -380,7 +380,7 @@ int u3dg_trainer_set_graphs(u3dg_trainer *trainer, int enable)
         TrainerImpl &t = impl(trainer);
         t.useGraphs = enable != 0;
         if (!t.useGraphs)
-            t.stepGraph.reset();
+            t.resetGraphs();
     });
 }
 
@@ -398,7 +398,7 @@ int u3dg_trainer_set_raster_schedule(u3dg_trainer *trainer, int forward_block, i
         t.ws.forwardBlock = forward_block;
         t.ws.forwardDepth = forward_depth;
         t.ws.backwardDepth = backward_depth;
-        t.stepGraph.reset(); // its kernels were recorded for the other depth
+        t.resetGraphs(); // its kernels were recorded for the other depth
     });
 }
 
@@ -408,7 +408,7 @@ int u3dg_trainer_set_tile_culling(u3dg_trainer *trainer, int enable)
         TrainerImpl &t = impl(trainer);
         t.finish();
         t.ws.cullTiles = enable != 0;
-        t.stepGraph.reset(); // its emission kernels were recorded with the other setting
+        t.resetGraphs(); // its emission kernels were recorded with the other setting
     });
 }
 

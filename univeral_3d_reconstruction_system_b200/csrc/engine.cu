@@ -344,8 +344,11 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     for (const u3dg_camera &c : cams)
         uniformViews = uniformViews && c.width == cams[0].width && c.height == cams[0].height;
     descDev.reserve(kGraphSteps, true);
-    descHost.reserve(kGraphSteps);
-    graphStatus.reserve(kGraphSteps);
+    descHost.reserve(2 * kGraphSteps);
+    statusDev.reserve(kGraphSteps, true);
+    graphStatus.reserve(2 * kGraphSteps);
+    for (cudaEvent_t &e : chunkDone)
+        U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     // Intersection buffers sized for 16 tiles per Gaussian at the capacity; they grow on demand.
     ws.reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * cap));
     // Everything a step or a densification needs, at the capacity: no allocation during a schedule
@@ -372,6 +375,9 @@ TrainerImpl::~TrainerImpl()
         cudaEventDestroy(f.done);
     for (cudaEvent_t e : freeEvents)
         cudaEventDestroy(e);
+    for (cudaEvent_t e : chunkDone)
+        if (e)
+            cudaEventDestroy(e);
     delete timer;
 }
 
@@ -439,14 +445,41 @@ void TrainerImpl::step()
 void TrainerImpl::stepTo(int target)
 {
     target = std::min(target, o.iterations);
+    // Graph runs are pipelined: the next run is launched (from the other slot) before the host waits
+    // for the previous one, so the GPU is not idle while the host checks statuses and prepares
+    // descriptors. A run that overflowed rolls the host state back to its failing step; the run
+    // launched after it did nothing on the device (the abort is sticky) and is dropped.
+    int pending = -1; // slot of the run launched but not yet checked
     while (iteration < target && !cams.empty()) {
         if (graphEligible(target)) {
-            finish(); // graph chunks start with no step in flight
-            if (graphEligible(target))
-                runGraphChunk(); // false: rolled back or not captured; the loop goes on from the restored state
+            if (pending < 0) {
+                finish(); // graph runs start with no single step in flight
+                if (!graphEligible(target))
+                    continue;
+            }
+            const int slot = pending < 0 ? 0 : 1 - pending;
+            const bool launched = beginGraphChunk(slot);
+            if (pending >= 0 && !endGraphChunk(pending, false)) {
+                if (launched)
+                    dropGraphChunk(slot);
+                pending = -1;
+                continue;
+            }
+            pending = launched ? slot : -1;
+            continue;
+        }
+        if (pending >= 0) { // the steps after the graph runs start from their checked state
+            endGraphChunk(pending, false);
+            pending = -1;
             continue;
         }
         step();
+    }
+    if (pending >= 0) {
+        const int last = pending;
+        pending = -1;
+        if (!endGraphChunk(last, false))
+            stepTo(target); // replay the rolled-back steps
     }
 }
 
@@ -536,7 +569,8 @@ void TrainerImpl::launchStep(const StepValues &sv, const StepDesc *desc, BinCoun
     U3DG_CUDA(cudaGetLastError());
     if (tm)
         tm->mark(6, stream);
-    U3DG_CUDA(cudaMemcpyAsync(statusDst, ws.counts.p, sizeof(BinCounts), cudaMemcpyDeviceToHost, stream));
+    // statusDst: pinned host memory (single steps) or device memory (graph runs).
+    U3DG_CUDA(cudaMemcpyAsync(statusDst, ws.counts.p, sizeof(BinCounts), cudaMemcpyDefault, stream));
 }
 
 void TrainerImpl::enqueueStep()
@@ -612,14 +646,15 @@ bool TrainerImpl::runGraphChunk()
     return endGraphChunk();
 }
 
-void TrainerImpl::prepareGraphChunk(StepValues *vals)
+void TrainerImpl::prepareGraphChunk(StepValues *vals, int slot)
 {
     constexpr int K = kGraphSteps;
-    pendingSnaps.assign(K, HostSnapshot{});
+    std::vector<HostSnapshot> &snaps = pendingSnaps[slot];
+    snaps.assign(K, HostSnapshot{});
     for (int k = 0; k < K; ++k) {
-        pendingSnaps[k] = snapshot();
+        snaps[k] = snapshot();
         vals[k] = nextStep();
-        descHost.p[k] = vals[k].d;
+        descHost.p[slot * K + k] = vals[k].d;
         ++iteration;
     }
 }
@@ -627,19 +662,33 @@ void TrainerImpl::prepareGraphChunk(StepValues *vals)
 void TrainerImpl::recordGraphChunk(const StepValues *vals)
 {
     for (int k = 0; k < kGraphSteps; ++k)
-        launchStep(vals[k], descDev.p + k, graphStatus.p + k);
+        launchStep(vals[k], descDev.p + k, statusDev.p + k);
     U3DG_CUDA(cudaMemcpyAsync(hStats.p, dStats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream));
 }
 
-void TrainerImpl::uploadGraphChunk(cudaStream_t s)
+void TrainerImpl::uploadGraphChunk(cudaStream_t s, int slot)
 {
-    U3DG_CUDA(cudaMemcpyAsync(descDev.p, descHost.p, kGraphSteps * sizeof(StepDesc), cudaMemcpyHostToDevice, s));
+    constexpr int K = kGraphSteps;
+    U3DG_CUDA(cudaMemcpyAsync(descDev.p, descHost.p + slot * K, K * sizeof(StepDesc), cudaMemcpyHostToDevice, s));
 }
 
-void TrainerImpl::abandonGraphChunk()
+void TrainerImpl::downloadGraphStatus(cudaStream_t s, int slot)
 {
-    restore(pendingSnaps[0]);
-    pendingSnaps.clear();
+    constexpr int K = kGraphSteps;
+    U3DG_CUDA(cudaMemcpyAsync(graphStatus.p + slot * K, statusDev.p, K * sizeof(BinCounts), cudaMemcpyDeviceToHost, s));
+}
+
+void TrainerImpl::abandonGraphChunk(int slot)
+{
+    restore(pendingSnaps[slot][0]);
+    pendingSnaps[slot].clear();
+}
+
+void TrainerImpl::dropGraphChunk(int slot)
+{
+    // The host state was already rolled back past this run; its device work did nothing (sticky
+    // abort), and the stream order puts any later work after it.
+    pendingSnaps[slot].clear();
 }
 
 // Makes `exec` run `graph`: an in-place update when the topology allows it, else a new instance.
@@ -659,11 +708,11 @@ static void applyGraph(cudaGraphExec_t &exec, cudaGraph_t graph)
         U3DG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
 }
 
-bool TrainerImpl::beginGraphChunk()
+bool TrainerImpl::beginGraphChunk(int slot)
 {
     constexpr int K = kGraphSteps;
     StepValues vals[K];
-    prepareGraphChunk(vals);
+    prepareGraphChunk(vals, slot);
     const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
                        stepGraph.icap != ws.icap || stepGraph.epoch != allocEpoch();
     if (stale) {
@@ -693,7 +742,7 @@ bool TrainerImpl::beginGraphChunk()
         if (allocEpoch() != epoch0) {
             // A buffer moved while the steps were being recorded: the graph may hold stale addresses.
             stepGraph.reset();
-            abandonGraphChunk();
+            abandonGraphChunk(slot);
             return false;
         }
         applyGraph(stepGraph.exec, stepGraph.graph);
@@ -703,23 +752,31 @@ bool TrainerImpl::beginGraphChunk()
         stepGraph.icap = ws.icap;
         stepGraph.epoch = allocEpoch();
     }
-    uploadGraphChunk(stream);
+    // One graph serves both slots: the device-side descriptors and statuses are rewritten and read
+    // in stream order, and each slot keeps its own host copies.
+    uploadGraphChunk(stream, slot);
     U3DG_CUDA(cudaGraphLaunch(stepGraph.exec, stream));
+    downloadGraphStatus(stream, slot);
+    U3DG_CUDA(cudaEventRecord(chunkDone[slot], stream));
     addLaunches(stepGraph.kernels);
     ++graphChunks;
     return true;
 }
 
-bool TrainerImpl::endGraphChunk()
+bool TrainerImpl::endGraphChunk(int slot, bool wholeStream)
 {
-    sync();
-    const int K = int(pendingSnaps.size());
+    if (wholeStream)
+        sync();
+    else
+        U3DG_CUDA(cudaEventSynchronize(chunkDone[slot]));
+    std::vector<HostSnapshot> &snaps = pendingSnaps[slot];
+    const int K = int(snaps.size());
     for (int k = 0; k < K; ++k) {
-        const BinCounts c = graphStatus.p[k];
+        const BinCounts c = graphStatus.p[slot * kGraphSteps + k];
         if (c.abortIter >= 0) {
-            // Step k overflowed: it and the steps after it did nothing on the device.
-            restore(pendingSnaps[k]);
-            pendingSnaps.clear();
+            // Step k overflowed: it and every step queued after it did nothing on the device.
+            restore(snaps[k]);
+            snaps.clear();
             ws.reserveIntersections(size_t(c.need) + size_t(c.need) / 2);
             ws.clearCounts(stream);
             ++replays;
@@ -728,7 +785,7 @@ bool TrainerImpl::endGraphChunk()
         if (size_t(c.total) + size_t(c.total) / 4 > size_t(ws.icap))
             ws.reserveIntersections(size_t(c.total) + size_t(c.total) / 2);
     }
-    pendingSnaps.clear();
+    snaps.clear();
     return true;
 }
 
@@ -816,6 +873,8 @@ static bool runCombinedRound(const std::vector<TrainerImpl *> &ts, BatchGraph &b
     for (TrainerImpl *t : ts)
         t->uploadGraphChunk(s0);
     U3DG_CUDA(cudaGraphLaunch(bg.exec, s0));
+    for (TrainerImpl *t : ts)
+        t->downloadGraphStatus(s0);
     addLaunches(bg.kernels);
     ++bg.launches;
     U3DG_CUDA(cudaStreamSynchronize(s0));

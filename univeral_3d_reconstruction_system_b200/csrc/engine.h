@@ -326,10 +326,17 @@ struct TrainerImpl {
     static constexpr int kGraphSteps = 10;
     bool useGraphs = true;
     bool uniformViews = false;
+    // Graph runs of kGraphSteps steps. A trainer keeps one run in flight while the host prepares and
+    // launches the next (stepTo), alternating two slots of host-side descriptors and statuses; the
+    // graph reads its descriptors from, and writes its statuses to, device buffers that each launch
+    // refills and copies out in stream order. Batches use slot 0.
     StepGraph stepGraph;
-    DevBuf<StepDesc> descDev;
-    HostPinned<StepDesc> descHost;
-    HostPinned<BinCounts> graphStatus;
+    DevBuf<StepDesc> descDev;          // kGraphSteps
+    HostPinned<StepDesc> descHost;     // 2 * kGraphSteps
+    DevBuf<BinCounts> statusDev;       // kGraphSteps
+    HostPinned<BinCounts> graphStatus; // 2 * kGraphSteps
+    cudaEvent_t chunkDone[2] = {nullptr, nullptr};
+    void resetGraphs() { stepGraph.reset(); }
     long long graphChunks = 0;        // graph launches so far
     long long normalSteps = 0;        // steps launched one by one (the first step is never a graph)
 
@@ -373,18 +380,26 @@ public:
     // runGraphChunk in two halves, so several trainers can have a chunk in flight at once: begin
     // advances the host state, captures the graph if stale and launches it (no wait; false when a
     // capture had to be discarded, with the state restored); end waits and checks the statuses.
-    bool beginGraphChunk();
-    bool endGraphChunk();
-    // The parts of beginGraphChunk, for a graph that holds several trainers' chunks (stepBatch):
+    // Launches the next 10 steps as one graph run in `slot` (false: nothing launched, the host state
+    // is back where it was). endGraphChunk waits for the slot's run (the whole stream when
+    // `wholeStream`) and checks its statuses; false means a step overflowed and the host state was
+    // rolled back to it (a run launched after it in the other slot then did nothing on the device and
+    // must be dropped with dropGraphChunk).
+    bool beginGraphChunk(int slot = 0);
+    bool endGraphChunk(int slot = 0, bool wholeStream = true);
+    void dropGraphChunk(int slot);
+    // The parts of beginGraphChunk, for a graph that holds several trainers' chunks (stepBatch, slot 0):
     // advance the host state by kGraphSteps steps, record their launches on this trainer's stream
     // (inside a capture), upload their descriptors on stream s, or undo the host-state advance.
-    void prepareGraphChunk(StepValues *vals);
+    void prepareGraphChunk(StepValues *vals, int slot = 0);
     void recordGraphChunk(const StepValues *vals);
-    void uploadGraphChunk(cudaStream_t s);
-    void abandonGraphChunk();
+    void uploadGraphChunk(cudaStream_t s, int slot = 0);
+    // After a launch: the run's statuses into the slot's host copy (stream order).
+    void downloadGraphStatus(cudaStream_t s, int slot = 0);
+    void abandonGraphChunk(int slot = 0);
 
 private:
-    std::vector<HostSnapshot> pendingSnaps; // host state before each step of the chunk in flight
+    std::vector<HostSnapshot> pendingSnaps[2]; // host state before each step of the slot's run
     // Checks the oldest queued step; returns false (after rolling back) when it had overflowed.
     bool checkOldest();
 };
