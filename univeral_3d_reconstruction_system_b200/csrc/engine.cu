@@ -12,8 +12,9 @@
 //
 // Runs of 10 steps with no densification or opacity reset among them go through a CUDA graph whose
 // kernels read each step's camera, target and learning rates from device descriptors (StepDesc); the
-// graph is recorded once and updated in place when the model size or buffers change. stepBatch runs
-// several trainers this way, as one graph launch per round when all of them can. Every buffer a
+// graph is recorded once and updated in place when the model size or buffers change. A trainer keeps
+// one run in flight while the host checks the previous one and prepares the next (stepTo). stepBatch
+// runs several trainers this way, as one graph launch per round when all of them can. Every buffer a
 // schedule needs is allocated when the trainer is created, so a schedule never waits on an allocation.
 
 #include "engine.h"
