@@ -7,7 +7,7 @@
 //
 // The constructors and fromReference/toReference helpers are templates over any type with the
 // reference's field names, so code holding the reference's own u3d::GaussianModel / TrainImage /
-// TrainOptions / RenderCamera can pass them straight in (see INTEGRATION.md).
+// TrainOptions / RenderCamera can pass them straight in.
 #pragma once
 
 #include "u3dg.h"

@@ -318,9 +318,11 @@ int u3dg_psnr(const float *a, const float *b, size_t count, float *out);
  * live in a fixed 11.1 MB device array per device, so width*height must be <= 640*480 and the image
  * at most 2048 loss blocks of 32x16 pixels; larger images return U3DG_ERR_CAPACITY. Work runs on
  * `stream` (a cudaStream_t; NULL = the default stream), and the call synchronises it before
- * returning. The first call on a device resolves the array's address there; make it before any
- * stream capture begins on that device. Calls on one device share the array and are serialised by
- * a per-device lock. Same results as u3dg_photometric_loss. */
+ * returning (it returns the loss values on the host). The first call in each device context (the
+ * first on a device, and the first after a cudaDeviceReset there) resolves the array's address in
+ * that context; make it before any stream capture begins on that device. Calls on one device share
+ * the array and are serialised by a per-device lock. out may be NULL. Same results as
+ * u3dg_photometric_loss. */
 int u3dg_photometric_loss_noalloc(const float *render, const float *target, int width, int height, float lambda,
                                   float *grad, u3dg_loss_value *out, void *stream);
 

@@ -712,6 +712,9 @@ static void applyGraph(cudaGraphExec_t &exec, cudaGraph_t graph)
 bool TrainerImpl::beginGraphChunk(int slot)
 {
     constexpr int K = kGraphSteps;
+    // This slot's pinned descriptors are rewritten below: its previous run (checked already, or dropped
+    // after an overflow without a wait) must have finished reading them.
+    U3DG_CUDA(cudaEventSynchronize(chunkDone[slot]));
     StepValues vals[K];
     prepareGraphChunk(vals, slot);
     const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
@@ -778,13 +781,18 @@ bool TrainerImpl::endGraphChunk(int slot, bool wholeStream)
             // Step k overflowed: it and every step queued after it did nothing on the device.
             restore(snaps[k]);
             snaps.clear();
+            if (!wholeStream)
+                sync(); // the next run, already queued, still uses the buffers about to be replaced
             ws.reserveIntersections(size_t(c.need) + size_t(c.need) / 2);
             ws.clearCounts(stream);
             ++replays;
             return false;
         }
-        if (size_t(c.total) + size_t(c.total) / 4 > size_t(ws.icap))
+        if (size_t(c.total) + size_t(c.total) / 4 > size_t(ws.icap)) {
+            if (!wholeStream)
+                sync();
             ws.reserveIntersections(size_t(c.total) + size_t(c.total) / 2);
+        }
     }
     snaps.clear();
     return true;

@@ -24,11 +24,16 @@ constexpr int kTW = 32, kTH = 16;        // output tile
 constexpr int kIW = kTW + 2 * kR, kIH = kTH + 2 * kR;
 constexpr int kThreads = 256;
 
-__constant__ float cWin[2 * kR + 1];
+// The 11 blur weights, passed to the loss kernels by value: kernel parameters sit in the constant
+// bank like a __constant__ array, but need no upload into each device context (no synchronous copy
+// before the first launch, nothing to redo after a context is recreated, nothing shared between host
+// threads), and a captured graph keeps them with the launch.
+struct SsimWindow {
+    float w[2 * kR + 1];
+};
 
 // The window exactly as Loss.cpp:15-27 builds it (host float arithmetic with glibc expf).
-struct HostWindow {
-    float w[2 * kR + 1];
+struct HostWindow : SsimWindow {
     HostWindow()
     {
         float sum = 0;
@@ -62,7 +67,7 @@ __device__ __forceinline__ double blockSumDouble(double v)
 __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *render, const float *targetF,
                                                               const uint8_t *targetU8, int W, int H, float lambda,
                                                               float *grad, float *abc, double *blockSums,
-                                                              const StepDesc *desc)
+                                                              const StepDesc *desc, const SsimWindow cWin)
 {
     if (desc)
         targetU8 = desc->target;
@@ -109,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *rende
                 float s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * kR; ++t) {
-                    const float a = sx[iy][ox + t], b = sy[iy][ox + t], w = cWin[t];
+                    const float a = sx[iy][ox + t], b = sy[iy][ox + t], w = cWin.w[t];
                     s0 += w * a;
                     s1 += w * b;
                     s2 += w * a * a;
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *rende
                 float m[5] = {0, 0, 0, 0, 0};
 #pragma unroll
                 for (int t = 0; t <= 2 * kR; ++t) {
-                    const float w = cWin[t];
+                    const float w = cWin.w[t];
 #pragma unroll
                     for (int j = 0; j < 5; ++j)
                         m[j] += w * hm[j][oy + t][ox];
@@ -165,7 +170,8 @@ __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *rende
 
 __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *render, const float *targetF,
                                                                const uint8_t *targetU8, int W, int H, const float *abc,
-                                                               float *grad, const StepDesc *desc)
+                                                               float *grad, const StepDesc *desc,
+                                                               const SsimWindow cWin)
 {
     if (desc)
         targetU8 = desc->target;
@@ -191,7 +197,7 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
             float a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
             for (int t = 0; t <= 2 * kR; ++t) {
-                const float w = cWin[t];
+                const float w = cWin.w[t];
                 a0 += w * sm[0][iy][ox + t];
                 a1 += w * sm[1][iy][ox + t];
                 a2 += w * sm[2][iy][ox + t];
@@ -210,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
             float g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
             for (int t = 0; t <= 2 * kR; ++t) {
-                const float w = cWin[t];
+                const float w = cWin.w[t];
                 g0 += w * hm[0][oy + t][ox];
                 g1 += w * hm[1][oy + t][ox];
                 g2 += w * hm[2][oy + t][ox];
@@ -313,20 +319,10 @@ __global__ void quantizeKernel(const float *rgb, size_t count, uint8_t *out)
     out[k] = uint8_t(r);
 }
 
-bool gWindowReady = false;
-
-void ensureWindow()
+const SsimWindow &window()
 {
-    // The constant is per device context; uploading it again is harmless and cheap.
-    static thread_local int lastDevice = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (gWindowReady && dev == lastDevice)
-        return;
-    const HostWindow w;
-    cudaMemcpyToSymbol(cWin, w.w, sizeof(w.w));
-    gWindowReady = true;
-    lastDevice = dev;
+    static const HostWindow w; // thread-safe one-time initialisation
+    return w;
 }
 
 constexpr int kSqBlocks = 296; // 2 x 148 SMs
@@ -338,12 +334,12 @@ int lossBlocks(int width, int height) { return ((width + kTW - 1) / kTW) * ((hei
 void launchLoss(const float *render, const float *targetF, const uint8_t *targetU8, int width, int height, float lambda,
                 float *grad, const LossScratch &ls, cudaStream_t s, const StepDesc *desc)
 {
-    ensureWindow();
+    const SsimWindow &win = window();
     dim3 g((width + kTW - 1) / kTW, (height + kTH - 1) / kTH);
     { lossForwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, lambda, grad, ls.abc,
-                                             ls.blockSums, desc); countLaunch(); }
+                                             ls.blockSums, desc, win); countLaunch(); }
     if (lambda > 0.0f)
-        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad, desc); countLaunch(); }
+        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad, desc, win); countLaunch(); }
 }
 
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,

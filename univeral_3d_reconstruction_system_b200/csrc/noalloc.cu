@@ -18,18 +18,25 @@
 // Limits: width * height <= kMaxPixels (640 x 480) and at most kMaxBlocks loss blocks (32 x 16
 // pixels each); larger requests are rejected with U3DG_ERR_CAPACITY before anything is launched.
 //
-// First-call set-up: the first call on a device, with that device current, resolves the array's
-// address there with cudaGetSymbolAddress (which loads this module into the context) and keeps it;
-// the loss window constant is uploaded on the first loss launch of each device and host thread. Make
-// that first call before any stream capture on that device begins.
+// Set-up: the first call in each device context, with that device current, resolves the array's
+// address there with cudaGetSymbolAddress (which loads this module into the context) and keeps it
+// with the context's id. A later call in a different context of that device (after cudaDeviceReset
+// destroyed the old one) resolves it again. Make the first call on a device, and the first after a
+// reset, before any stream capture on that device begins.
 //
 // Overlapping calls: all calls on one device share the one scratch array. Each call holds a
 // per-device lock from its first launch until it has synchronised `stream`, so calls from several
 // host threads run one after another instead of overwriting each other's scratch; two processes have
 // separate contexts and separate copies of the array.
+//
+// The call returns the loss values on the host, so it waits for `stream` to finish the loss before
+// it returns (and before it releases the lock); the four result floats are read back on `stream`
+// into the caller's stack, which needs no pinned buffer because the wait follows at once.
 
 #include "engine.h"
 #include "kernels.h"
+
+#include <cudaTypedefs.h>
 
 #include <mutex>
 
@@ -48,7 +55,28 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double gNoAllocScratch[kScratchDoubles];
 
 std::mutex gDeviceLock[kMaxDevices];
-double *gScratchAddress[kMaxDevices] = {}; // set once per device, under that device's lock
+// The array's address in each device's context, and the id of the context it was resolved in; read
+// and written under that device's lock.
+double *gScratchAddress[kMaxDevices] = {};
+unsigned long long gScratchContext[kMaxDevices] = {};
+
+// Id of the calling thread's current context (cuCtxGetId through the runtime's driver entry point);
+// 0 when no context is current yet.
+unsigned long long currentContextId()
+{
+    static PFN_cuCtxGetId getId = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuCtxGetId>(fn);
+    }();
+    if (!getId)
+        throw StatusError(U3DG_ERR_CUDA, "cuCtxGetId is not available from the CUDA driver");
+    unsigned long long id = 0;
+    return getId(nullptr, &id) == CUDA_SUCCESS ? id : 0;
+}
 
 } // namespace
 
@@ -69,10 +97,18 @@ extern "C" int u3dg_photometric_loss_noalloc(const float *render, const float *t
         if (device < 0 || device >= kMaxDevices)
             throw StatusError(U3DG_ERR_INVALID_ARG, "device index out of range");
         std::lock_guard<std::mutex> lock(gDeviceLock[device]);
-        if (!gScratchAddress[device]) {
+        unsigned long long ctx = currentContextId();
+        if (ctx == 0) {
+            U3DG_CUDA(cudaSetDevice(device)); // creates and binds the device's primary context (CUDA 12)
+            ctx = currentContextId();
+            if (ctx == 0)
+                throw StatusError(U3DG_ERR_CUDA, "no CUDA context is current on the device");
+        }
+        if (!gScratchAddress[device] || gScratchContext[device] != ctx) {
             void *p = nullptr;
             U3DG_CUDA(cudaGetSymbolAddress(&p, gNoAllocScratch));
             gScratchAddress[device] = static_cast<double *>(p);
+            gScratchContext[device] = ctx;
         }
         double *base = gScratchAddress[device];
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -82,7 +118,8 @@ extern "C" int u3dg_photometric_loss_noalloc(const float *render, const float *t
         launchLossFinalize(ls, width, height, lambda, nullptr, 0, nullptr, vals, vals + 3, s);
         U3DG_CUDA(cudaGetLastError());
         float v[4] = {0, 0, 0, 0};
-        U3DG_CUDA(cudaMemcpyAsync(v, vals, sizeof(v), cudaMemcpyDeviceToHost, s));
+        if (out)
+            U3DG_CUDA(cudaMemcpyAsync(v, vals, sizeof(v), cudaMemcpyDeviceToHost, s));
         U3DG_CUDA(cudaStreamSynchronize(s));
         if (out) {
             out->total = v[0];
