@@ -1,5 +1,6 @@
-// host_io.cpp - host-side Gaussian model I/O (binary 3DGS PLY) and the plain point-cloud
-// initialisation. These run once per training run, outside the hot loop.
+// host_io.cpp - the plain point-cloud initialisation on the host (its hash grid is shared with the
+// GPU neighbour search in init.cu). Runs once per training run, outside the hot loop. The PLY
+// reader and writer are in ply.cpp.
 
 #include "host_io.h"
 
@@ -120,335 +121,6 @@ void initGaussiansFromPointsHost(const float *xyz, const float *rgb, size_t n, u
                 }
     }
     finishInitFromNeighbours(xyz, rgb, n, g.cell, best.data(), out);
-}
-
-// ------------------------------------------------------------------ PLY
-
-namespace {
-
-bool fail(std::string *error, const std::string &m)
-{
-    if (error)
-        *error = m;
-    return false;
-}
-
-enum class PType { I8, U8, I16, U16, I32, U32, F32, F64, Bad };
-
-PType typeOf(const std::string &t)
-{
-    static const std::pair<const char *, PType> names[] = {
-        {"char", PType::I8},   {"int8", PType::I8},     {"uchar", PType::U8},  {"uint8", PType::U8},
-        {"short", PType::I16}, {"int16", PType::I16},   {"ushort", PType::U16}, {"uint16", PType::U16},
-        {"int", PType::I32},   {"int32", PType::I32},   {"uint", PType::U32},  {"uint32", PType::U32},
-        {"float", PType::F32}, {"float32", PType::F32}, {"double", PType::F64}, {"float64", PType::F64}};
-    for (const auto &p : names)
-        if (t == p.first)
-            return p.second;
-    return PType::Bad;
-}
-
-int sizeOf(PType t)
-{
-    switch (t) {
-    case PType::I8:
-    case PType::U8: return 1;
-    case PType::I16:
-    case PType::U16: return 2;
-    case PType::I32:
-    case PType::U32:
-    case PType::F32: return 4;
-    case PType::F64: return 8;
-    default: return 0;
-    }
-}
-
-struct Prop {
-    std::string name;
-    PType type = PType::Bad, countType = PType::Bad;
-    bool list = false;
-};
-
-struct Elem {
-    std::string name;
-    size_t count = 0;
-    std::vector<Prop> props;
-};
-
-enum class Fmt { Ascii, LE, BE };
-
-bool littleEndianHost()
-{
-    const uint16_t v = 1;
-    uint8_t b;
-    std::memcpy(&b, &v, 1);
-    return b == 1;
-}
-
-// Sequential value reader over the PLY body.
-struct Body {
-    const char *p, *end;
-    Fmt fmt;
-    bool value(PType t, double &out)
-    {
-        if (fmt == Fmt::Ascii) {
-            while (p < end && std::isspace(static_cast<unsigned char>(*p)))
-                ++p;
-            const char *s = p;
-            while (p < end && !std::isspace(static_cast<unsigned char>(*p)))
-                ++p;
-            if (p == s)
-                return false;
-            std::istringstream ss(std::string(s, p));
-            ss.imbue(std::locale::classic());
-            ss >> out;
-            return !ss.fail();
-        }
-        const int sz = sizeOf(t);
-        if (sz == 0 || end - p < sz)
-            return false;
-        unsigned char b[8];
-        std::memcpy(b, p, size_t(sz));
-        p += sz;
-        if ((fmt == Fmt::LE) != littleEndianHost())
-            std::reverse(b, b + sz);
-        switch (t) {
-        case PType::I8: { int8_t v; std::memcpy(&v, b, 1); out = v; break; }
-        case PType::U8: out = b[0]; break;
-        case PType::I16: { int16_t v; std::memcpy(&v, b, 2); out = v; break; }
-        case PType::U16: { uint16_t v; std::memcpy(&v, b, 2); out = v; break; }
-        case PType::I32: { int32_t v; std::memcpy(&v, b, 4); out = v; break; }
-        case PType::U32: { uint32_t v; std::memcpy(&v, b, 4); out = v; break; }
-        case PType::F32: { float v; std::memcpy(&v, b, 4); out = v; break; }
-        case PType::F64: { double v; std::memcpy(&v, b, 8); out = v; break; }
-        default: return false;
-        }
-        return true;
-    }
-    bool skip(const Prop &q)
-    {
-        double v;
-        if (!q.list)
-            return fmt == Fmt::Ascii ? value(q.type, v) : advance(sizeOf(q.type));
-        double c;
-        if (!value(q.countType, c) || c < 0)
-            return false;
-        for (size_t k = 0; k < size_t(c); ++k)
-            if (!(fmt == Fmt::Ascii ? value(q.type, v) : advance(sizeOf(q.type))))
-                return false;
-        return true;
-    }
-    bool advance(int n)
-    {
-        if (end - p < n)
-            return false;
-        p += n;
-        return true;
-    }
-};
-
-// Reads the vertex table: one row of `wanted.size()` values per vertex (NaN where missing).
-bool readVertices(const std::string &path, const std::vector<std::string> &wanted, std::vector<float> &rows,
-                  std::vector<bool> &found, size_t &count, std::string *error)
-{
-    std::ifstream in(path, std::ios::binary);
-    if (!in)
-        return fail(error, "Cannot open " + path);
-    std::vector<char> data((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
-    const std::string head(data.data(), std::min<size_t>(data.size(), 1 << 16));
-    if (head.compare(0, 3, "ply") != 0)
-        return fail(error, "Not a PLY file: " + path);
-    const size_t endHeader = head.find("end_header");
-    if (endHeader == std::string::npos)
-        return fail(error, "PLY header has no end_header");
-    const size_t bodyStart = head.find('\n', endHeader);
-    if (bodyStart == std::string::npos)
-        return fail(error, "Truncated PLY header");
-    Fmt fmt = Fmt::Ascii;
-    std::vector<Elem> elems;
-    std::istringstream hs(head.substr(0, endHeader));
-    std::string line;
-    while (std::getline(hs, line)) {
-        std::istringstream ls(line);
-        std::string w;
-        ls >> w;
-        if (w == "format") {
-            std::string f;
-            ls >> f;
-            if (f == "ascii")
-                fmt = Fmt::Ascii;
-            else if (f == "binary_little_endian")
-                fmt = Fmt::LE;
-            else if (f == "binary_big_endian")
-                fmt = Fmt::BE;
-            else
-                return fail(error, "Unknown PLY format " + f);
-        } else if (w == "element") {
-            Elem e;
-            ls >> e.name >> e.count;
-            elems.push_back(e);
-        } else if (w == "property" && !elems.empty()) {
-            Prop q;
-            std::string a, b, c;
-            ls >> a >> b >> c;
-            if (a == "list") {
-                q.list = true;
-                q.countType = typeOf(b);
-                q.type = typeOf(c);
-                ls >> q.name;
-            } else {
-                q.type = typeOf(a);
-                q.name = b;
-            }
-            if (q.type == PType::Bad)
-                return fail(error, "Unsupported PLY property: " + line);
-            elems.back().props.push_back(q);
-        }
-    }
-    Body body{data.data() + bodyStart + 1, data.data() + data.size(), fmt};
-    for (const Elem &e : elems) {
-        if (e.name != "vertex") {
-            for (size_t i = 0; i < e.count; ++i)
-                for (const Prop &q : e.props)
-                    if (!body.skip(q))
-                        return fail(error, "Truncated PLY data");
-            continue;
-        }
-        std::vector<int> column(e.props.size(), -1);
-        found.assign(wanted.size(), false);
-        for (size_t k = 0; k < wanted.size(); ++k)
-            for (size_t q = 0; q < e.props.size(); ++q)
-                if (!e.props[q].list && e.props[q].name == wanted[k]) {
-                    column[q] = int(k);
-                    found[k] = true;
-                }
-        count = e.count;
-        rows.assign(e.count * wanted.size(), std::nanf(""));
-        for (size_t i = 0; i < e.count; ++i)
-            for (size_t q = 0; q < e.props.size(); ++q) {
-                if (column[q] < 0) {
-                    if (!body.skip(e.props[q]))
-                        return fail(error, "Truncated PLY data at vertex " + std::to_string(i));
-                    continue;
-                }
-                double v;
-                if (!body.value(e.props[q].type, v))
-                    return fail(error, "Truncated PLY data at vertex " + std::to_string(i));
-                const std::string &name = wanted[size_t(column[q])];
-                if (name == "red" || name == "green" || name == "blue") {
-                    if (e.props[q].type == PType::U8)
-                        v /= 255.0;
-                    else if (e.props[q].type == PType::U16)
-                        v /= 65535.0;
-                }
-                rows[i * wanted.size() + size_t(column[q])] = float(v);
-            }
-        return true;
-    }
-    return fail(error, "PLY file has no vertex element");
-}
-
-void putFloatLE(std::ofstream &out, float v)
-{
-    unsigned char b[4];
-    std::memcpy(b, &v, 4);
-    if (!littleEndianHost())
-        std::reverse(b, b + 4);
-    out.write(reinterpret_cast<const char *>(b), 4);
-}
-
-} // namespace
-
-bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error)
-{
-    std::ofstream out(path, std::ios::binary);
-    if (!out)
-        return fail(error, "Cannot write " + path);
-    static const char *props[] = {"x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2", "opacity",
-                                  "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"};
-    out << "ply\nformat binary_little_endian 1.0\n";
-    out << "comment Universal 3D Reconstruction System\n";
-    out << "element vertex " << m.count << "\n";
-    for (const char *p : props)
-        out << "property float " << p << "\n";
-    out << "end_header\n";
-    for (size_t i = 0; i < m.count; ++i) {
-        for (int k = 0; k < 3; ++k)
-            putFloatLE(out, m.means[i * 3 + k]);
-        for (int k = 0; k < 3; ++k)
-            putFloatLE(out, 0.0f);
-        for (int k = 0; k < 3; ++k)
-            putFloatLE(out, m.colors[i * 3 + k]);
-        putFloatLE(out, m.opacities[i]);
-        for (int k = 0; k < 3; ++k)
-            putFloatLE(out, m.scales[i * 3 + k]);
-        for (int k = 0; k < 4; ++k)
-            putFloatLE(out, m.quats[i * 4 + k]);
-    }
-    if (!out)
-        return fail(error, "Write error: " + path);
-    return true;
-}
-
-bool readSplatPlyHost(const std::string &path, HostModel &model, std::string *error, bool *isSplat)
-{
-    const std::vector<std::string> wanted = {"x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2", "opacity", "scale_0",
-                                             "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3", "red",
-                                             "green", "blue"};
-    std::vector<float> rows;
-    std::vector<bool> found;
-    size_t count = 0;
-    if (!readVertices(path, wanted, rows, found, count, error))
-        return false;
-    if (!found[0] || !found[1] || !found[2])
-        return fail(error, "PLY vertices have no x/y/z");
-    const bool splat = found[3] && found[6] && found[7] && found[10];
-    if (isSplat)
-        *isSplat = splat;
-    const size_t W = wanted.size();
-    if (!splat) {
-        // A plain point cloud becomes small opaque Gaussians (SplatPly.cpp:301-321).
-        std::vector<float> xyz, rgb;
-        for (size_t i = 0; i < count; ++i) {
-            const float *r = &rows[i * W];
-            if (!std::isfinite(r[0]) || !std::isfinite(r[1]) || !std::isfinite(r[2]))
-                continue;
-            xyz.insert(xyz.end(), {r[0], r[1], r[2]});
-            if (found[14])
-                rgb.insert(rgb.end(), {r[14], r[15], r[16]});
-            else
-                rgb.insert(rgb.end(), {0.8f, 0.8f, 0.8f});
-        }
-        const size_t n = xyz.size() / 3;
-        model.resize(n);
-        u3dg_model v{model.means.data(), model.scales.data(), model.quats.data(), model.opac.data(),
-                     model.colors.data(), n};
-        initGaussiansFromPointsHost(xyz.data(), rgb.data(), n, v);
-        const float o = logitHost(0.95f), ls = std::log(0.5f);
-        for (float &x : model.opac)
-            x = o;
-        for (float &s : model.scales)
-            s += ls;
-        return true;
-    }
-    model.resize(count);
-    size_t out = 0;
-    for (size_t i = 0; i < count; ++i) {
-        const float *r = &rows[i * W];
-        if (!std::isfinite(r[0]) || !std::isfinite(r[1]) || !std::isfinite(r[2]))
-            continue;
-        for (int k = 0; k < 3; ++k) {
-            model.means[out * 3 + k] = r[k];
-            model.colors[out * 3 + k] = r[3 + k];
-            model.scales[out * 3 + k] = r[7 + k];
-        }
-        model.opac[out] = r[6];
-        for (int k = 0; k < 4; ++k)
-            model.quats[out * 4 + k] = r[10 + k];
-        ++out;
-    }
-    model.resize(out);
-    return true;
 }
 
 } // namespace u3dg
