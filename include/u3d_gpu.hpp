@@ -202,7 +202,10 @@ public:
         for (std::size_t k = 0; k < m_images.size(); ++k)
             views[k] = {m_images[k].camera, m_images[k].rgb.data()};
         const u3dg_model v = initial.view();
-        check(u3dg_trainer_create(&v, views.data(), int(views.size()), sceneExtent, &m_options, &m_t));
+        // The trainer owns its images (as the reference's does), so they can go to the GPU while
+        // the first steps run.
+        check(u3dg_trainer_create_background_upload(&v, views.data(), int(views.size()), sceneExtent, &m_options,
+                                                    &m_t));
     }
 
     ~Trainer() { u3dg_trainer_destroy(m_t); }

@@ -166,6 +166,20 @@ void u3dg_train_options_for_iterations(int iterations, u3dg_train_options *out);
  * Device buffers are sized once for options->max_gaussians (at least initial->count). */
 int u3dg_trainer_create(const u3dg_model *initial, const u3dg_image *images, int image_count,
                         float scene_extent, const u3dg_train_options *options, u3dg_trainer **out);
+/* Trainer::Trainer as u3dg_trainer_create, except that the images are copied to the GPU by a host
+ * thread while the first steps already run: views are sent in the order the first epoch uses them
+ * and each step waits (on the GPU) only for its own view, so a short run does not wait for every
+ * image first. Results are identical to u3dg_trainer_create's. The caller's pixel buffers
+ * (images[k].rgb) must stay valid and unchanged until u3dg_trainer_wait_uploads returns or the
+ * trainer is destroyed; the image array itself and the model may be freed on return. (The
+ * reference's Trainer owns its images, which it takes by value: a caller that keeps them alive
+ * beside the trainer, as the C++ drop-in does, loses nothing.) */
+int u3dg_trainer_create_background_upload(const u3dg_model *initial, const u3dg_image *images, int image_count,
+                                          float scene_extent, const u3dg_train_options *options,
+                                          u3dg_trainer **out);
+/* Blocks until every image of a trainer created with background upload is on the GPU; afterwards
+ * the caller may release its pixel buffers. Returns at once for other trainers. */
+int u3dg_trainer_wait_uploads(u3dg_trainer *trainer);
 /* Trainer::step (Trainer.cpp:53-103), `count` times. Returns without work once done, like the
  * reference. The work is queued on the trainer's CUDA stream; only densification steps wait
  * for the GPU (they read back the split count to draw the split samples on the host). */
@@ -253,6 +267,12 @@ int u3dg_rasterizer_tiles(u3dg_rasterizer *r, int *tiles_x, int *tiles_y, int *o
                           int *list, size_t list_capacity, size_t *list_length);
 /* Per-pixel state of the last forward (m_finalT, m_nContrib, Rasterizer.h:82-84). */
 int u3dg_rasterizer_pixel_state(u3dg_rasterizer *r, float *final_t, int *n_contrib, size_t pixels);
+/* No reference counterpart (the trainers' tile culling at the unit boundary): with enable = 1 the
+ * following forwards list each Gaussian only in the tiles of its rectangle that its contributing
+ * ellipse (alpha >= min_alpha) can reach, as the trainers do by default; every tile list is then an
+ * order-preserving subsequence of Rasterizer::binTiles' list (Rasterizer.cpp:206-261) and images,
+ * pixel state and gradients are unchanged. 0 (the default) keeps the reference's lists. */
+int u3dg_rasterizer_set_tile_culling(u3dg_rasterizer *r, int enable);
 void u3dg_rasterizer_destroy(u3dg_rasterizer *r);
 
 /* Tile binning of Rasterizer::binTiles (Rasterizer.cpp:206-261) on the GPU, from given projected
@@ -280,7 +300,7 @@ int u3dg_densify_and_prune(u3dg_model *model, u3dg_model *adam_m, u3dg_model *ad
  * and options[s] (each with its own schedule and Gaussian cap). Every scene keeps its own trainer and
  * stream; u3dg_batch_step advances each scene by `count` iterations (or to its end), interleaving the
  * scenes so their kernels run concurrently and running steps through each scene's step graph where
- * it can. With autotune != 0, each scene's tile size (8 or 16) and compositing schedule (the
+ * it can. With autotune != 0, each scene's tile size (8, 16 or 32) and compositing schedule (the
  * settings of u3dg_trainer_set_raster_schedule; same results for any) are chosen at creation from
  * short timed runs on throwaway trainers; tile_size reports the tile and the tuned ms per step (0
  * without autotune), schedule the compositing settings as well. batch_trainer

@@ -1,5 +1,6 @@
 """Batched multi-scene training (u3dg_batch_*): every scene of a batch trains exactly as the same scene
-trained alone, with or without the autotuner of tile size and compositing schedule."""
+trained alone, with or without the autotuner of tile size and compositing schedule, at tile 16 and at
+tile 32 (four backward CTAs per tile with separate partial slots: deterministic)."""
 from __future__ import annotations
 
 import dataclasses
@@ -36,9 +37,12 @@ def _alone(u3dg, scene, tile, raster, iterations):
     return t.model().flat(), t.stats()
 
 
-@pytest.mark.parametrize("autotune", [False, True])
-def test_batch_matches_scenes_trained_alone(u3dg, autotune):
+@pytest.mark.parametrize("autotune,tile", [(False, 16), (False, 32), (True, 0)])
+def test_batch_matches_scenes_trained_alone(u3dg, autotune, tile):
     scenes = _scenes(u3dg)
+    if tile:
+        scenes = [(i, im, e, dataclasses.replace(o, raster=dataclasses.replace(o.raster, tile_size=tile)))
+                  for i, im, e, o in scenes]
     b = u3dg.Batch(scenes, autotune=autotune)
     assert len(b) == 3
     b.step(77)
@@ -51,9 +55,9 @@ def test_batch_matches_scenes_trained_alone(u3dg, autotune):
         tile, tuned = b.tile_size(k)
         tile2, raster, tuned2 = b.schedule(k)
         assert (tile2, tuned2) == (tile, tuned)
-        assert tile in (8, 16) and raster[0] in (8, 16) and raster[1] in (1, 2) and raster[2] in (1, 2)
+        assert tile in (8, 16, 32) and raster[0] in (8, 16) and raster[1] in (1, 2) and raster[2] in (1, 2)
         if not autotune:
-            assert (tile, raster, tuned) == (16, (8, 1, 1), 0.0)
+            assert (tile, raster, tuned) == (scene[3].raster.tile_size, (8, 1, 1), 0.0)
         else:
             assert tuned > 0
         t = b.trainer(k)

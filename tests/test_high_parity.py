@@ -1,0 +1,113 @@
+"""One High-preset step against the CPU oracle at full size: 640x480, 300k and 250k Gaussians.
+
+The unit-boundary rasterizer runs the trainers' configuration (tile culling on, 8x8 forward CTAs,
+persistent heaviest-first backward) on the High scene's first view, and the oracle (the reference's
+Rasterizer restated, Rasterizer.cpp:137-545) runs the same projection, binning, compositing and
+backward. Checked per step, as one training step computes them:
+  - tile lists and their depth order: bit-exact against binTiles on identical projected records
+    (the 300k depth sort and ~2.5M intersections), and with culling on, every tile's list is an
+    order-preserving subsequence of the reference's list for that tile;
+  - image within 1e-5 absolute per channel, final transmittance within 1e-5, contributor counts exact;
+  - per-parameter gradients of the L1 + 0.2 D-SSIM loss against the view's target within 1e-4
+    relative (floor: 1% of the group's largest magnitude) and the NDC densification statistic.
+Models: the bench workload (initGaussiansFromPoints of every true centre plus 50k re-samples:
+isotropic, opacity 0.1) and the ground truth itself (anisotropic, opacity 0.3-1)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from helpers import grad_close
+from univeral_3d_reconstruction_system_b200.scenes import dense_init_points, make_scene
+from univeral_3d_reconstruction_system_b200.types import RasterSettings, TrainImage
+
+pytestmark = pytest.mark.gpu
+
+GROUPS = ("means", "scales", "quats", "opacities", "colors")
+THREADS = max(1, min(os.cpu_count() or 1, 32))
+
+
+@pytest.fixture(scope="module")
+def high(oracle):
+    sc = make_scene("high", 0)
+    st = RasterSettings()
+    cam = sc.cameras[0]
+    target = TrainImage.quantize(oracle.render(sc.truth, cam, st, sc.sh_rest, 3, threads=THREADS))
+    return sc, cam, target.astype(np.float32) / np.float32(255.0)
+
+
+@pytest.fixture(scope="module", params=["bench-300k", "truth-250k"])
+def model(request, high, oracle):
+    sc = high[0]
+    if request.param == "truth-250k":
+        return sc.truth
+    xyz, rgb = dense_init_points(sc, 300_000)
+    return oracle.init_from_points(xyz, rgb)
+
+
+def _subsequence_lists(off, lst, roff, rlst, n):
+    """Every tile's list in (off, lst) is an order-preserving subsequence of its list in (roff, rlst)."""
+    tiles = len(roff) - 1
+    rt = np.repeat(np.arange(tiles, dtype=np.int64), np.diff(roff))
+    rkey = rt * n + rlst.astype(np.int64)  # unique per (tile, Gaussian), increasing position in rlst
+    order = np.argsort(rkey, kind="stable")
+    t = np.repeat(np.arange(tiles, dtype=np.int64), np.diff(off))
+    key = t * n + lst.astype(np.int64)
+    idx = np.searchsorted(rkey[order], key)
+    assert np.all(idx < len(rkey)) and np.array_equal(rkey[order][np.minimum(idx, len(rkey) - 1)], key), \
+        "a culled list holds an entry the reference's list does not"
+    pos = order[idx]  # position of each culled entry in the reference list
+    same_tile = t[1:] == t[:-1]
+    assert np.all(pos[1:][same_tile] > pos[:-1][same_tile]), "culled lists changed the depth order"
+
+
+def test_high_step_matches_oracle(u3dg, oracle, high, model):
+    sc, cam, target = high
+    st = RasterSettings()
+    n = model.size()
+    o = oracle.raster(THREADS)
+    ref_img = o.forward(model, cam, st)
+    ref_off, ref_list = o.tiles()
+    ref_ft, ref_nc = o.pixel_state()
+    assert len(ref_list) > 1_000_000
+
+    # Tile lists bit-exact on identical projected records (the full-size depth sort and bucketing).
+    p = o.projection()
+    tx, ty = (cam.width + 15) // 16, (cam.height + 15) // 16
+    g_off, g_list = u3dg.binTiles(p["depth"], p["radius"], p["rect"], tx, ty)
+    np.testing.assert_array_equal(g_off, ref_off)
+    np.testing.assert_array_equal(g_list, ref_list)
+
+    # The trainers' configuration: culled lists, 8x8 forward CTAs.
+    r = u3dg.Rasterizer()
+    r.set_tile_culling(True)
+    img = r.forward(model, cam, st)
+    assert float(np.max(np.abs(img - ref_img))) <= 1e-5
+    ft, nc = r.pixel_state()
+    np.testing.assert_array_equal(nc, ref_nc)
+    assert float(np.max(np.abs(ft - ref_ft))) <= 1e-5
+    off, lst = r.tiles()
+    assert len(lst) < len(ref_list)
+    _subsequence_lists(off, lst, ref_off, ref_list, n)
+
+    # The step's loss gradient (oracle's loss on the oracle's image), through both backward passes.
+    _, dl = oracle.photometric_loss(ref_img, target, cam.width, cam.height, 0.2)
+    dl = dl.reshape(ref_img.shape)
+    ndc = np.zeros(n, np.float32)
+    g = r.backward(model, dl, None, ndc)
+    og, ondc = o.backward(dl)
+    for name in GROUPS:
+        ok, worst = grad_close(getattr(g, name), getattr(og, name), rel=1e-4)
+        assert ok, (name, worst)
+    ok, worst = grad_close(ndc, ondc, rel=1e-4)
+    assert ok, ("ndc", worst)
+
+    # Culling off at the unit boundary: the reference's own lists.
+    r.set_tile_culling(False)
+    img2 = r.forward(model, cam, st)
+    np.testing.assert_array_equal(img2, img)
+    off2, lst2 = r.tiles()
+    np.testing.assert_array_equal(off2, ref_off)
+    np.testing.assert_array_equal(lst2, ref_list)

@@ -96,3 +96,40 @@ def test_two_ranks_share_the_label_scenes(tmp_path):
     x0, t0 = got[0][1]
     expect = [float(s) for s in range(10, 17) for _ in range(3 + s % 4)]
     assert x0 == expect and t0 == [-v for v in expect]
+
+
+def _batched_rank(rank: int, world: int, port: int, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from univeral_3d_reconstruction_system_b200.scenes import batched_specs
+    d = bench.Dist(world, backend="gloo")
+    try:
+        specs = batched_specs(0, 16)
+        mine = bench.batched_shard(len(specs), d.world, d.rank)
+        iters = sum(specs[k].iterations for k in mine)
+        # Per-rank device times and PSNR differences as a rank would measure them.
+        got = bench.combine_batched(d, iters, 100.0 + 10 * rank, 300.0 - 50 * rank, 0.01 * rank)
+        q.put((rank, mine, iters, got))
+    finally:
+        d.close()
+
+
+def test_two_ranks_split_the_batched_scenes():
+    """The batched leg with two gloo ranks: rank r trains scenes r, r + 2, ... (disjoint, covering all
+    16), and every rank ends with the whole job's iteration count and the slowest rank's times."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batched_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = dict((r, rest) for r, *rest in (q.get(timeout=5) for _ in range(2)))
+    assert got[0][0] == list(range(0, 16, 2)) and got[1][0] == list(range(1, 16, 2))
+    total = got[0][1] + got[1][1]
+    for r in (0, 1):
+        assert got[r][2] == (total, 110.0, 300.0, 0.01)

@@ -43,6 +43,8 @@ SIGNATURES = {
     "u3dg_train_options_default": (None, [_OPT]),
     "u3dg_train_options_for_iterations": (None, [C.c_int, _OPT]),
     "u3dg_trainer_create": (C.c_int, [_MV, C.POINTER(_abi.Image), C.c_int, C.c_float, _OPT, _PP]),
+    "u3dg_trainer_create_background_upload": (C.c_int, [_MV, C.POINTER(_abi.Image), C.c_int, C.c_float, _OPT, _PP]),
+    "u3dg_trainer_wait_uploads": (C.c_int, [_P]),
     "u3dg_trainer_step": (C.c_int, [_P, C.c_int]),
     "u3dg_trainer_done": (C.c_int, [_P, _I]),
     "u3dg_trainer_iteration": (C.c_int, [_P, _I]),
@@ -71,6 +73,7 @@ SIGNATURES = {
     "u3dg_rasterizer_projection": (C.c_int, [_P, C.c_size_t, _F, _F, _F, _F, _F, _F, _I, _abi.u8p]),
     "u3dg_rasterizer_tiles": (C.c_int, [_P, _I, _I, _I, C.c_size_t, _I, C.c_size_t, _SZ]),
     "u3dg_rasterizer_pixel_state": (C.c_int, [_P, _F, _I, C.c_size_t]),
+    "u3dg_rasterizer_set_tile_culling": (C.c_int, [_P, C.c_int]),
     "u3dg_rasterizer_destroy": (None, [_P]),
     "u3dg_bin_tiles": (C.c_int, [_F, _I, _I, C.c_size_t, C.c_int, C.c_int, _I, _I, C.c_size_t, _SZ]),
     "u3dg_densify_and_prune": (C.c_int, [_MV, _MV, _MV, _F, _I, C.c_size_t, C.c_float, _OPT, C.c_int, C.c_uint,

@@ -35,7 +35,9 @@ class Trainer:
     """GPU drop-in for u3d::Trainer. `pool` is accepted for API compatibility and ignored."""
 
     def __init__(self, initial: GaussianModel, images, scene_extent: float, options: TrainOptions | None = None,
-                 pool=None):
+                 pool=None, background_upload: bool = False):
+        """background_upload: images go to the GPU on a host thread while the first steps run
+        (u3dg_trainer_create_background_upload); the trainer keeps the pixel arrays alive."""
         L = load()
         self._images = list(images)
         self._options = options or TrainOptions()
@@ -43,10 +45,15 @@ class Trainer:
         iv = initial.view()
         opt = self._options.struct()
         h = C.c_void_p()
-        check(L.u3dg_trainer_create(C.byref(iv), arr, len(self._images), float(scene_extent), C.byref(opt),
-                                    C.byref(h)))
+        create = L.u3dg_trainer_create_background_upload if background_upload else L.u3dg_trainer_create
+        check(create(C.byref(iv), arr, len(self._images), float(scene_extent), C.byref(opt), C.byref(h)))
         self._h = h
-        del keep
+        # The pixel arrays the C side reads (contiguous copies where needed) live as long as the trainer.
+        self._keep = keep if background_upload else None
+
+    def wait_uploads(self) -> None:
+        """Blocks until every training image is on the GPU (background upload)."""
+        check(load().u3dg_trainer_wait_uploads(self._h))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -312,6 +319,11 @@ class Rasterizer:
         nc = np.zeros(P, np.int32)
         check(load().u3dg_rasterizer_pixel_state(self._h, _abi.fptr(ft), _abi.iptr(nc), P))
         return ft, nc
+
+    def set_tile_culling(self, enable: bool) -> None:
+        """List each Gaussian only in the tiles its contributing ellipse reaches (the trainers'
+        default); the lists become subsequences of the reference's, results are unchanged."""
+        check(load().u3dg_rasterizer_set_tile_culling(self._h, 1 if enable else 0))
 
 
 def binTiles(depth, radius, rect, tiles_x: int, tiles_y: int):

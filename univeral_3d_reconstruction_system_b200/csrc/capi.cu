@@ -197,12 +197,33 @@ int u3dg_trainer_create(const u3dg_model *initial, const u3dg_image *images, int
     });
 }
 
+int u3dg_trainer_create_background_upload(const u3dg_model *initial, const u3dg_image *images, int image_count,
+                                          float scene_extent, const u3dg_train_options *options,
+                                          u3dg_trainer **out)
+{
+    return guarded([&] {
+        if (!out || !options)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "options and out must not be NULL");
+        *out = nullptr;
+        requireModel(initial, "initial model");
+        requireDevice();
+        auto t = std::make_unique<u3dg_trainer>();
+        t->impl = std::make_unique<TrainerImpl>(*initial, images, image_count, scene_extent, *options, true);
+        *out = t.release();
+    });
+}
+
 static TrainerImpl &impl(u3dg_trainer *t)
 {
     if (!t || !t->impl)
         throw StatusError(U3DG_ERR_INVALID_ARG, "trainer is NULL");
     U3DG_CUDA(cudaSetDevice(t->impl->device));
     return *t->impl;
+}
+
+int u3dg_trainer_wait_uploads(u3dg_trainer *trainer)
+{
+    return guarded([&] { impl(trainer).waitUploads(); });
 }
 
 int u3dg_trainer_step(u3dg_trainer *trainer, int count)
@@ -432,6 +453,9 @@ int u3dg_trainer_time_steps(u3dg_trainer *trainer, int count, float *ms)
         U3DG_CUDA(cudaEventCreate(&a));
         U3DG_CUDA(cudaEventCreate(&b));
         t.finish();
+        // The first run's graph is recorded before the timed region (recording executes nothing).
+        if (count > 0)
+            t.primeGraph(t.iteration + count);
         U3DG_CUDA(cudaEventRecord(a, t.stream));
         if (count > 0)
             t.stepTo(t.iteration + count);
@@ -634,6 +658,15 @@ int u3dg_rasterizer_pixel_state(u3dg_rasterizer *r, float *final_t, int *n_contr
         if (n_contrib)
             U3DG_CUDA(cudaMemcpyAsync(n_contrib, R.ws.nContrib.p, P * sizeof(int), cudaMemcpyDeviceToHost, R.stream.s));
         R.stream.sync();
+    });
+}
+
+int u3dg_rasterizer_set_tile_culling(u3dg_rasterizer *r, int enable)
+{
+    return guarded([&] {
+        u3dg_rasterizer &R = rz(r);
+        R.ws.cullTiles = enable != 0;
+        R.haveForward = false; // the next backward needs a forward with the new lists
     });
 }
 

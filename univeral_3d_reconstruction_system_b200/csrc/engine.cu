@@ -107,7 +107,7 @@ void RasterWorkspace::reserveIntersections(size_t capacity)
     iVals1.reserve(capacity, true);
     emitGid.reserve(capacity, true);
     list.reserve(capacity, true);
-    partial.reserve(capacity * kG2d, true);
+    partial.reserve(capacity * kG2d * size_t(partialSlots), true);
     icap = int(capacity);
 }
 
@@ -125,6 +125,11 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     reserveGaussians(nn);
     if (icap == 0)
         reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * nn));
+    const int per = st.tile_size > 16 ? st.tile_size / 16 : 1;
+    if (per * per > partialSlots) { // a tile size spanning more backward CTAs than before
+        partialSlots = per * per;
+        partial.reserve(size_t(icap) * kG2d * size_t(partialSlots), true);
+    }
     ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
     launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
 }
@@ -213,8 +218,13 @@ RasterArgs RasterWorkspace::rasterArgs() const
     a.minAlpha = st.min_alpha;
     a.minTransmittance = st.min_transmittance;
     const int pb = st.tile_size <= 8 ? 8 : 16;
-    a.blocksX = (cam.width + pb - 1) / pb;
-    a.blocksY = (cam.height + pb - 1) / pb;
+    // Whole tiles of pixel blocks: a block past the image edge composites nothing, but (for tiles of
+    // several blocks) still writes its slot of every entry of its tile.
+    const int per = st.tile_size > pb ? st.tile_size / pb : 1;
+    a.blocksX = tilesX * per;
+    a.blocksY = tilesY * per;
+    a.subSlots = per * per;
+    a.subStride = size_t(icap) * kG2d;
     a.blockOrder = blockOrder.p;
     a.counters = blockCounters.p;
     a.forwardBlock = forwardBlock;
@@ -230,7 +240,8 @@ void RasterWorkspace::composite(cudaStream_t stream)
     finalT.reserve(P);
     nContrib.reserve(P);
     const int pb = st.tile_size <= 8 ? 8 : 16;
-    blockOrder.reserve(size_t(std::max(1, ((cam.width + pb - 1) / pb) * ((cam.height + pb - 1) / pb))));
+    const int per = st.tile_size > pb ? st.tile_size / pb : 1;
+    blockOrder.reserve(size_t(std::max(1, tilesX * per * tilesY * per)));
     const RasterArgs a = rasterArgs();
     launchBlockOrder(a, blockOrder.p, stream);
     launchCompositeForward(a, rgb.p, finalT.p, nContrib.p, stream);
@@ -238,8 +249,6 @@ void RasterWorkspace::composite(cudaStream_t stream)
 
 void RasterWorkspace::backwardComposite(const float *dLdRgb, cudaStream_t stream)
 {
-    if (st.tile_size > 16)
-        U3DG_CUDA(cudaMemsetAsync(partial.p, 0, size_t(icap) * kG2d * sizeof(float), stream));
     launchCompositeBackward(rasterArgs(), dLdRgb, finalT.p, nContrib.p, partial.p, stream);
 }
 
@@ -257,6 +266,9 @@ ChainArgs RasterWorkspace::chainArgs(const Params &P) const
     a.offs = offs.p;
     a.sortedIds = sortedIds;
     a.partial = partial.p;
+    const int per = st.tile_size > 16 ? st.tile_size / 16 : 1;
+    a.subSlots = per * per;
+    a.subStride = size_t(icap) * kG2d;
     a.g2d = g2d.p;
     a.counts = counts.p;
     return a;
@@ -290,7 +302,7 @@ static void copyArenaToModel(const float *base, size_t cap, size_t n, u3dg_model
 }
 
 TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int count, float sceneExtent,
-                         const u3dg_train_options &opt)
+                         const u3dg_train_options &opt, bool backgroundUpload)
     : o(opt), rng(opt.seed)
 {
     checkSettings(o.raster);
@@ -329,9 +341,12 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
         maxP = std::max(maxP, P);
     }
     images.reserve(std::max<size_t>(total, 1), true);
-    for (int k = 0; k < count; ++k) {
-        const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
-        U3DG_CUDA(cudaMemcpyAsync(images.p + imageOffset[size_t(k)], imgs[k].rgb, P * 3, cudaMemcpyHostToDevice, stream));
+    if (!backgroundUpload || count == 0) {
+        for (int k = 0; k < count; ++k) {
+            const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
+            U3DG_CUDA(cudaMemcpyAsync(images.p + imageOffset[size_t(k)], imgs[k].rgb, P * 3, cudaMemcpyHostToDevice,
+                                      stream));
+        }
     }
     dLoss.reserve(maxP * 3);
     abc.reserve(maxP * 9);
@@ -362,12 +377,110 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     hCounts.reserve(4);
     hNormals.reserve(6 * cap);
     normals.reserve(6 * cap);
-    // The host buffers of the caller may be released after this call returns.
+    if (backgroundUpload && count > 0)
+        startUploads(imgs, count);
+    // The model's host buffers may be released after this call returns (and the images' too, unless
+    // they are uploaded in the background).
     U3DG_CUDA(cudaStreamSynchronize(stream));
+}
+
+void TrainerImpl::startUploads(const u3dg_image *imgs, int count)
+{
+    auto up = std::make_unique<ImageUploader>();
+    U3DG_CUDA(cudaStreamCreateWithFlags(&up->copy, cudaStreamNonBlocking));
+    up->ready.assign(size_t(count), nullptr);
+    for (cudaEvent_t &e : up->ready)
+        U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    up->waited.assign(size_t(count), 0);
+    // The first epoch's view order, as nextStep will draw it from the same generator state.
+    std::vector<int> first(static_cast<size_t>(count));
+    for (int k = 0; k < count; ++k)
+        first[size_t(k)] = k;
+    std::mt19937 r = rng;
+    std::shuffle(first.begin(), first.end(), r);
+    up->position.assign(size_t(count), 0);
+    for (int k = 0; k < count; ++k)
+        up->position[size_t(first[size_t(k)])] = k;
+    std::vector<const uint8_t *> src(static_cast<size_t>(count));
+    for (int k = 0; k < count; ++k)
+        src[size_t(k)] = imgs[k].rgb;
+    ImageUploader *u = up.get();
+    const int dev = device;
+    uint8_t *dst = images.p;
+    std::vector<size_t> offsets = imageOffset, bytes(static_cast<size_t>(count));
+    for (int k = 0; k < count; ++k)
+        bytes[size_t(k)] = size_t(imgs[k].camera.width) * imgs[k].camera.height * 3;
+    up->thread = std::thread([u, dev, dst, first, src, offsets, bytes] {
+        std::string err;
+        if (cudaSetDevice(dev) != cudaSuccess)
+            err = "cudaSetDevice failed in the image upload thread";
+        for (size_t k = 0; k < first.size() && err.empty(); ++k) {
+            const size_t v = size_t(first[k]);
+            cudaError_t e = cudaMemcpyAsync(dst + offsets[v], src[v], bytes[v], cudaMemcpyHostToDevice, u->copy);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(u->ready[v], u->copy);
+            if (e != cudaSuccess) {
+                err = std::string("image upload: ") + cudaGetErrorString(e);
+                break;
+            }
+            std::lock_guard<std::mutex> lock(u->m);
+            u->issued = int(k) + 1;
+            u->cv.notify_all();
+        }
+        std::lock_guard<std::mutex> lock(u->m);
+        if (!err.empty())
+            u->error = err;
+        u->cv.notify_all();
+    });
+    uploader = std::move(up);
+}
+
+void TrainerImpl::requireView(size_t v)
+{
+    ImageUploader *u = uploader.get();
+    if (!u || u->waited[v])
+        return;
+    {
+        std::unique_lock<std::mutex> lock(u->m);
+        u->cv.wait(lock, [&] { return u->issued > u->position[v] || !u->error.empty(); });
+        if (u->issued <= u->position[v])
+            throw StatusError(U3DG_ERR_CUDA, u->error);
+    }
+    U3DG_CUDA(cudaStreamWaitEvent(stream, u->ready[v], 0));
+    u->waited[v] = 1;
+}
+
+void TrainerImpl::waitUploads()
+{
+    ImageUploader *u = uploader.get();
+    if (!u || u->joined)
+        return;
+    if (u->thread.joinable())
+        u->thread.join();
+    u->joined = true;
+    U3DG_CUDA(cudaStreamSynchronize(u->copy));
+    if (!u->error.empty())
+        throw StatusError(U3DG_ERR_CUDA, u->error);
+    // Every image is in place: later steps need not wait for anything.
+    for (size_t v = 0; v < u->waited.size(); ++v)
+        if (!u->waited[v]) {
+            U3DG_CUDA(cudaStreamWaitEvent(stream, u->ready[v], 0));
+            u->waited[v] = 1;
+        }
 }
 
 TrainerImpl::~TrainerImpl()
 {
+    if (uploader) {
+        // The copies read the caller's buffers and write `images`: finish them first.
+        if (uploader->thread.joinable())
+            uploader->thread.join();
+        cudaStreamSynchronize(uploader->copy);
+        for (cudaEvent_t e : uploader->ready)
+            if (e)
+                cudaEventDestroy(e);
+        cudaStreamDestroy(uploader->copy);
+    }
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
@@ -512,6 +625,7 @@ StepValues TrainerImpl::nextStep()
         orderPos = 0;
     }
     sv.view = size_t(order[orderPos++]);
+    requireView(sv.view);
     sv.d.cam = cams[sv.view];
     sv.d.target = images.p + imageOffset[sv.view];
     sv.d.iteration = iteration;
@@ -709,6 +823,72 @@ static void applyGraph(cudaGraphExec_t &exec, cudaGraph_t graph)
         U3DG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
 }
 
+bool TrainerImpl::graphStale() const
+{
+    return stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur || stepGraph.icap != ws.icap ||
+           stepGraph.epoch != allocEpoch();
+}
+
+bool TrainerImpl::captureStepGraph(const StepValues *vals)
+{
+    // Keep the instantiated graph: a re-capture with the same topology (only kernel arguments and
+    // grid sizes change after a densification) updates it in place, cheaper than instantiating.
+    if (stepGraph.graph) {
+        cudaGraphDestroy(stepGraph.graph);
+        stepGraph.graph = nullptr;
+    }
+    const unsigned long long epoch0 = allocEpoch();
+    const unsigned long long launches0 = launchCount();
+    U3DG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    try {
+        recordGraphChunk(vals);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream, &g);
+        if (g)
+            cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    U3DG_CUDA(cudaStreamEndCapture(stream, &stepGraph.graph));
+    // The captured kernels ran no work yet: count them when the graph runs.
+    stepGraph.kernels = (long long)(launchCount() - launches0);
+    addLaunches(-stepGraph.kernels);
+    if (allocEpoch() != epoch0) {
+        // A buffer moved while the steps were being recorded: the graph may hold stale addresses.
+        stepGraph.reset();
+        return false;
+    }
+    applyGraph(stepGraph.exec, stepGraph.graph);
+    ++stepGraph.captures;
+    stepGraph.n = n;
+    stepGraph.cur = cur;
+    stepGraph.icap = ws.icap;
+    stepGraph.epoch = allocEpoch();
+    return true;
+}
+
+void TrainerImpl::primeGraph(int target)
+{
+    if (!graphEligible(target) || !graphStale())
+        return;
+    // Record the next run's graph with the values its steps would have, then put the host state back:
+    // a capture executes nothing, so the run itself later launches the same graph unchanged.
+    const HostSnapshot s = snapshot();
+    StepValues vals[kGraphSteps];
+    for (int k = 0; k < kGraphSteps; ++k) {
+        vals[k] = nextStep();
+        ++iteration;
+    }
+    try {
+        captureStepGraph(vals);
+    } catch (...) {
+        restore(s);
+        throw;
+    }
+    restore(s);
+}
+
 bool TrainerImpl::beginGraphChunk(int slot)
 {
     constexpr int K = kGraphSteps;
@@ -717,44 +897,9 @@ bool TrainerImpl::beginGraphChunk(int slot)
     U3DG_CUDA(cudaEventSynchronize(chunkDone[slot]));
     StepValues vals[K];
     prepareGraphChunk(vals, slot);
-    const bool stale = stepGraph.exec == nullptr || stepGraph.n != n || stepGraph.cur != cur ||
-                       stepGraph.icap != ws.icap || stepGraph.epoch != allocEpoch();
-    if (stale) {
-        // Keep the instantiated graph: a re-capture with the same topology (only kernel arguments and
-        // grid sizes change after a densification) updates it in place, cheaper than instantiating.
-        if (stepGraph.graph) {
-            cudaGraphDestroy(stepGraph.graph);
-            stepGraph.graph = nullptr;
-        }
-        const unsigned long long epoch0 = allocEpoch();
-        const unsigned long long launches0 = launchCount();
-        U3DG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
-        try {
-            recordGraphChunk(vals);
-        } catch (...) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(stream, &g);
-            if (g)
-                cudaGraphDestroy(g);
-            cudaGetLastError();
-            throw;
-        }
-        U3DG_CUDA(cudaStreamEndCapture(stream, &stepGraph.graph));
-        // The captured kernels ran no work yet: count them when the graph runs.
-        stepGraph.kernels = (long long)(launchCount() - launches0);
-        addLaunches(-stepGraph.kernels);
-        if (allocEpoch() != epoch0) {
-            // A buffer moved while the steps were being recorded: the graph may hold stale addresses.
-            stepGraph.reset();
-            abandonGraphChunk(slot);
-            return false;
-        }
-        applyGraph(stepGraph.exec, stepGraph.graph);
-        ++stepGraph.captures;
-        stepGraph.n = n;
-        stepGraph.cur = cur;
-        stepGraph.icap = ws.icap;
-        stepGraph.epoch = allocEpoch();
+    if (graphStale() && !captureStepGraph(vals)) {
+        abandonGraphChunk(slot);
+        return false;
     }
     // One graph serves both slots: the device-side descriptors and statuses are rewritten and read
     // in stream order, and each slot keeps its own host copies.
@@ -963,10 +1108,9 @@ void stepBatch(const std::vector<TrainerImpl *> &trainers, int count, BatchGraph
 RasterSchedule autotuneSchedule(const u3dg_model &initial, const u3dg_image *imgs, int count, float extent,
                                 const u3dg_train_options &opt)
 {
-    // Deterministic tile sizes only: tile 32 spans four CTAs per tile that add their partial
-    // gradients atomically, and two runs of one scene then differ (up to 0.35 dB after a 2000-iteration
-    // schedule with densification was measured).
-    static const int kTiles[2] = {16, 8};
+    // Every candidate is deterministic: tile 32 spans four backward CTAs per tile, each with its own
+    // partial slots, added in a fixed order by the chain rule.
+    static const int kTiles[3] = {16, 8, 32};
     RasterSchedule best{opt.raster.tile_size, 8, 1, 1, 0.0f};
     for (int tile : kTiles) {
         // Two runs per tile: forward 16x16 blocks at depth 1 with the backward at depth 1, and forward
@@ -1092,6 +1236,7 @@ void TrainerImpl::resetOpacity()
 float TrainerImpl::evaluatePsnr()
 {
     finish();
+    waitUploads();
     if (cams.empty())
         return 0.0f;
     constexpr int kSq = 297; // sqDiff partial blocks + 1 (loss.cu)

@@ -3,11 +3,14 @@
 
 #include "kernels.h"
 
+#include <condition_variable>
 #include <cstdio>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace u3dg {
@@ -151,8 +154,9 @@ struct RasterWorkspace {
     DevBuf<uint32_t> iKeys0, iKeys1, iVals0, iVals1;
     DevBuf<int> emitGid, list;
     uint32_t *listEmit = nullptr; // emission index per tile-sorted entry (one of iVals0 / iVals1)
-    DevBuf<float> partial;
+    DevBuf<float> partial;             // partialSlots arrays of icap * 9 floats
     int icap = 0;
+    int partialSlots = 1;              // slot arrays the backward needs: (tile size / 16)^2 above 16
     // per tile / pixel
     DevBuf<int> tileOffsets, nContrib;
     DevBuf<int> blockOrder, blockCounters; // compositing schedule: pixel blocks by list length, counters
@@ -274,6 +278,25 @@ struct InFlight {
     int slot = 0; // pinned status slot
 };
 
+// Training images copied to the device by a host thread while training starts (trainers created
+// with background upload). Views are copied in the order the first epoch will use them (the first
+// shuffle of the view order, computed from a copy of the trainer's generator), each on the copy
+// stream followed by an event; a step makes its stream wait for its view's event first, so no step
+// reads an image before it has arrived and the results are the same as with images uploaded at
+// creation.
+struct ImageUploader {
+    std::thread thread;
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t> ready; // per view
+    std::vector<int> position;      // per view: its place in the upload order
+    std::vector<char> waited;       // per view: the trainer's stream already waits for it
+    std::mutex m;
+    std::condition_variable cv;
+    int issued = 0;                 // copies issued so far, in upload order (guarded by m)
+    std::string error;              // first failure of the thread (guarded by m)
+    bool joined = false;
+};
+
 // The GPU Trainer (Trainer.h:47-93, Trainer.cpp).
 struct TrainerImpl {
     int device = 0;
@@ -340,9 +363,17 @@ struct TrainerImpl {
     long long graphChunks = 0;        // graph launches so far
     long long normalSteps = 0;        // steps launched one by one (the first step is never a graph)
 
+    // backgroundUpload: the images are copied by a host thread while the first steps run (the
+    // caller's pixel buffers must stay valid until waitUploads() returns or the trainer is gone).
     TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int count, float sceneExtent,
-                const u3dg_train_options &opt);
+                const u3dg_train_options &opt, bool backgroundUpload = false);
     ~TrainerImpl();
+    // Blocks until every image is on the device (no-op without background upload); afterwards the
+    // caller's pixel buffers may be released.
+    void waitUploads();
+    std::unique_ptr<ImageUploader> uploader;
+    // Makes the trainer's stream wait until view v's image has arrived (background upload).
+    void requireView(size_t v);
 
     Params params() { return paramsAt(arena[cur].p, cap); }
     Params moment1() { return paramsAt(arena[cur].p + 14 * cap, cap); }
@@ -364,6 +395,7 @@ struct TrainerImpl {
     void sync();
 
 private:
+    void startUploads(const u3dg_image *imgs, int count);
     HostSnapshot snapshot() const;
     void restore(const HostSnapshot &s);
     void enqueueStep();
@@ -386,6 +418,14 @@ public:
     // rolled back to it (a run launched after it in the other slot then did nothing on the device and
     // must be dropped with dropGraphChunk).
     bool beginGraphChunk(int slot = 0);
+    // Whether the step graph must be recorded again before its next launch.
+    bool graphStale() const;
+    // Records (and instantiates) the step graph for steps with these values; false when a buffer moved
+    // during the recording (the graph is dropped).
+    bool captureStepGraph(const StepValues *vals);
+    // Records the graph the next run toward `target` will launch, without running anything and with
+    // the host state unchanged (so a timed run does not include the recording).
+    void primeGraph(int target);
     bool endGraphChunk(int slot = 0, bool wholeStream = true);
     void dropGraphChunk(int slot);
     // The parts of beginGraphChunk, for a graph that holds several trainers' chunks (stepBatch, slot 0):

@@ -179,9 +179,9 @@ __device__ __forceinline__ void adamOne(float &p, float &m, float &v, float g, f
 // entry j of the chunk; a segmented inclusive scan over the lanes (segments = ranks) adds the entries
 // of each rank in lane order, and each rank's lane adds the scan value at its last entry in the chunk.
 // The order of the additions is fixed, so the sums are deterministic. Written per Gaussian id.
-__global__ void __launch_bounds__(256) partialSumKernel(const float *partial, const int *offs,
-                                                        const uint32_t *sortedIds, int n, const BinCounts *counts,
-                                                        float *g2d)
+__global__ void __launch_bounds__(256) partialSumKernel(const float *partial, int subSlots, size_t subStride,
+                                                        const int *offs, const uint32_t *sortedIds, int n,
+                                                        const BinCounts *counts, float *g2d)
 {
     if (counts != nullptr && counts->abortIter >= 0)
         return;
@@ -212,6 +212,13 @@ __global__ void __launch_bounds__(256) partialSumKernel(const float *partial, co
 #pragma unroll
             for (int k = 0; k < kG2d; ++k)
                 v[k] = in ? partial[size_t(e) * kG2d + k] : 0.0f;
+            // Tiles covered by several CTAs: their slots, added in slot order.
+            for (int sl = 1; sl < subSlots; ++sl) {
+                const float *p = partial + size_t(sl) * subStride;
+#pragma unroll
+                for (int k = 0; k < kG2d; ++k)
+                    v[k] = __fadd_rn(v[k], in ? p[size_t(e) * kG2d + k] : 0.0f);
+            }
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const int ownerUp = __shfl_up_sync(0xffffffffu, owner, d);
@@ -591,7 +598,7 @@ void launchChain(const ChainArgs &a, bool adam, cudaStream_t s)
     if (a.n <= 0)
         return;
     { partialSumKernel<<<std::min(blocks((long long)(a.n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(
-          a.partial, a.offs, a.sortedIds, a.n, a.counts, a.g2d); countLaunch(); }
+          a.partial, std::max(a.subSlots, 1), a.subStride, a.offs, a.sortedIds, a.n, a.counts, a.g2d); countLaunch(); }
     if (adam)
         { chainKernel<true><<<blocks(a.n, 256), 256, 0, s>>>(a); countLaunch(); }
     else

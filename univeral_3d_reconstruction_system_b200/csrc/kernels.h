@@ -51,7 +51,9 @@ struct ChainArgs {
     const int *rankOf;    // depth rank of every Gaussian
     const int *offs;      // per rank: first intersection in emission order (n + 1 entries)
     const uint32_t *sortedIds; // Gaussian id per depth rank
-    const float *partial; // per intersection, in emission order: 9 summed 2D gradients
+    const float *partial; // per intersection, in emission order: 9 summed 2D gradients (subSlots arrays)
+    int subSlots;         // slot arrays of partial (RasterArgs::subSlots), subStride floats apart
+    size_t subStride;
     float *g2d;           // per Gaussian: the 9 partials summed (written by launchChain's first kernel)
     const BinCounts *counts; // the kernel does nothing when counts->abortIter >= 0
     float *gradAccum;     // |dL/dmean2d| NDC statistic (may be null)
@@ -145,12 +147,18 @@ struct RasterArgs {
     int forwardBlock;      // pixel block edge of the forward kernel: 8 or 16 (tiles > 8 only; same results)
     int forwardDepth;      // list entries staged per thread per batch, forward: 1 or 2 (same results)
     int backwardDepth;     // the same for the backward kernel
+    // Tiles larger than the backward's 16x16 pixel block are covered by several CTAs: each writes its
+    // sums into its own slot array (slot = the block's position in its tile, row-major), subSlots
+    // arrays of subStride floats apart, and the chain rule adds a Gaussian's slots in slot order.
+    int subSlots;
+    size_t subStride;
 };
 // Orders the pixel blocks by the list length of their tile, longest first (log-scale buckets), into
 // order[blocksX * blocksY].
 void launchBlockOrder(const RasterArgs &a, int *order, cudaStream_t s);
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s);
-// partial: 9 floats per intersection in emission order; zeroed by the caller when tileSize > 16.
+// partial: 9 floats per intersection in emission order, in a.subSlots slot arrays (every slot of every
+// entry is written: no zeroing needed).
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
                              float *partial, cudaStream_t s);
 

@@ -8,7 +8,9 @@
 // per-warp shared-memory slot, and are added over the warps in warp order after the batch: the result
 // does not depend on scheduling. Each (tile, Gaussian) partial is stored once at the entry's emission
 // index, zero for entries behind every pixel's last contributor; the chain-rule kernel sums a
-// Gaussian's partials in tile order.
+// Gaussian's partials in tile order. Tiles of 32 or 64 pixels span 4 or 16 CTAs (16x16 blocks): each
+// stores into its own slot array and the chain-rule kernel adds the slots in a fixed order, so every
+// tile size gives deterministic gradients (no atomics).
 //
 // Contribution decisions (power, alpha, the cut-offs) and the transmittance recovery are computed with
 // explicitly unfused operations, exactly as in the forward, so the backward visits the same entries;
@@ -147,7 +149,7 @@ __device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix
 template <int PB, int BD>
 __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int by, const float *dLdRgb,
                                               const float *finalTIn, const int *nContribIn, float *partial,
-                                              int useAtomics, float4 *sP, float4 *sQ, float4 *sR,
+                                              float4 *sP, float4 *sQ, float4 *sR,
                                               uint32_t (*mask)[RasterShape<PB, BD>::NG], int &sMax, float *sWarp)
 {
     using S = RasterShape<PB, BD>;
@@ -157,6 +159,10 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     const int tile = tileOf<PB>(a, bx, by);
     const int start = a.tileOffsets[tile], end = a.tileOffsets[tile + 1];
     const bool in0 = wb.px < a.width && wb.py0 < a.height, in1 = wb.px < a.width && wb.py1 < a.height;
+    if (a.subSlots > 1) { // this block's slot array: its position in the tile, row-major
+        const int per = a.tileSize / PB;
+        partial += size_t((by % per) * per + bx % per) * a.subStride;
+    }
     PixelState s0, s1;
     initPixel(s0, in0, in0 ? size_t(wb.py0) * a.width + wb.px : 0, float(wb.py0), dLdRgb, finalTIn, nContribIn, a.bg);
     initPixel(s1, in1, in1 ? size_t(wb.py1) * a.width + wb.px : 0, float(wb.py1), dLdRgb, finalTIn, nContribIn, a.bg);
@@ -177,8 +183,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     // Entries behind every pixel's last contributor get no gradient (the reference's per-tile
     // accumulators start at zero); their partials are still written, as the chain-rule kernel sums
     // every intersection of a Gaussian.
-    if (!useAtomics)
-        for (int j = jmax + tid; j < end - start; j += NT) {
+    for (int j = jmax + tid; j < end - start; j += NT) {
             float *dst = partial + size_t(a.listEmit[start + j]) * kG2d;
 #pragma unroll
             for (int k = 0; k < kG2d; ++k)
@@ -251,15 +256,9 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                     sum[q] += sWarp[(size_t(w) * NB + e) * kG2d + q];
             finishEntry(sQ[e], sum);
             float *dst = partial + size_t(a.listEmit[start + bStart + e]) * kG2d;
-            if (useAtomics) {
 #pragma unroll
-                for (int q = 0; q < kG2d; ++q)
-                    atomicAdd(dst + q, sum[q]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < kG2d; ++q)
-                    dst[q] = sum[q];
-            }
+            for (int q = 0; q < kG2d; ++q)
+                dst[q] = sum[q];
         }
     }
 }
@@ -278,8 +277,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
 template <int PB, int BD>
 __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
                                                                               const float *finalTIn,
-                                                                              const int *nContribIn, float *partial,
-                                                                              int useAtomics)
+                                                                              const int *nContribIn, float *partial)
 {
     using S = RasterShape<PB, BD>;
     constexpr int NB = S::NB, NW = S::NW, NG = S::NG;
@@ -292,8 +290,8 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) comp
     const int units = a.blocksX * a.blocksY;
     int *counter = a.counters + 2; // backward: counters[2..3]
     for (int b = nextBlock(a, counter, &sNext); b < units; b = nextBlock(a, counter, &sNext))
-        backwardBlock<PB, BD>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, useAtomics, sP,
-                              sQ, sR, mask, sMax, sWarp);
+        backwardBlock<PB, BD>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, sP, sQ, sR,
+                              mask, sMax, sWarp);
 }
 
 template <class K>
@@ -321,8 +319,7 @@ static void launchBackward(const RasterArgs &a, const float *dLdRgb, const float
         return residentCtas(compositeBackwardKernel<PB, BD>, S::NT, smem);
     }();
     const int units = a.blocksX * a.blocksY;
-    { compositeBackwardKernel<PB, BD><<<std::min(units, ctas), S::NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial,
-                                                                          a.tileSize > PB ? 1 : 0); countLaunch(); }
+    { compositeBackwardKernel<PB, BD><<<std::min(units, ctas), S::NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial); countLaunch(); }
 }
 
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
