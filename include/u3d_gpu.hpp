@@ -12,10 +12,15 @@
 
 #include "u3dg.h"
 
+#include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdint>
-#include <stdexcept>
 #include <cstdio>
+#include <random>
+#include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -259,6 +264,8 @@ public:
         rgb.resize(std::size_t(c.width) * c.height * 3);
         check(u3dg_trainer_render(m_t, &c, rgb.data()));
     }
+    // The C ABI handle (for entry points with no reference counterpart, e.g. the PLY export).
+    u3dg_trainer *handle() const { return m_t; }
 
 private:
     template <class Image>
@@ -342,6 +349,111 @@ inline float psnr(const float *a, const float *b, std::size_t count)
     float p = 0;
     check(u3dg_psnr(a, b, count, &p));
     return p;
+}
+
+// ------------------------------------------------------------------ pipeline training stage
+
+// The training stage of reconstructProject (engine/src/pipeline/Reconstructor.cpp:296-361) on the GPU
+// trainer: scene extent, random initial points for sparse clouds, training cameras scaled to the
+// training images, initGaussiansFromPoints, the training loop with cancellation and progress, the
+// splat PLY and the mean training PSNR. Templated over the reference's types: Cam is u3d::Camera
+// (center(), scaled()), Img its TrainImage (camera, rgb); report / say / cancelled are the pipeline's
+// progress, log and cancel hooks (Progress-like objects with stage, fraction, message; strings;
+// bool()). The caller keeps the steps around it (loading, poses, alignment, cameras.txt and
+// sparse.ply, which need the cameras and points this updates in place).
+struct StageResult {
+    std::string splatPath;
+    std::size_t gaussians = 0;
+    float psnr = 0;
+    double extent = 0;
+};
+
+template <class Cam, class Img, class Report, class Say, class Cancelled>
+bool trainSplatStage(const std::vector<Cam> &cameras, std::vector<Img> &train, const std::vector<int> &fullWidth,
+                     std::vector<float> &xyz, std::vector<float> &rgb, int iterations, int maxGaussians,
+                     double trainStart, const std::string &splatPath, Report report, Say say, Cancelled cancelled,
+                     StageResult &result, std::string *error = nullptr)
+{
+    auto fail = [&](const std::string &m) {
+        if (error)
+            *error = m;
+        return false;
+    };
+    auto format = [](const char *fmt, double a = 0, double b = 0, double c = 0, double d = 0) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, fmt, a, b, c, d);
+        return std::string(buf);
+    };
+    if (cameras.empty() || cameras.size() != train.size() || fullWidth.size() != train.size())
+        return fail("Training needs one camera and one full-resolution width per image.");
+    // Extent: 1.1 x the largest camera distance from the mean camera centre (Reconstructor.cpp:288-296).
+    double mean[3] = {0, 0, 0};
+    for (const Cam &c : cameras) {
+        const auto cc = c.center();
+        for (int k = 0; k < 3; ++k)
+            mean[k] += cc[k] / double(cameras.size());
+    }
+    double extent = 0;
+    for (const Cam &c : cameras) {
+        const auto cc = c.center();
+        const double dx = cc[0] - mean[0], dy = cc[1] - mean[1], dz = cc[2] - mean[2];
+        extent = std::max(extent, std::sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    extent = std::max(extent * 1.1, 1e-3);
+    // Too few points: 10,000 random ones in a cube of 0.6 x extent (Reconstructor.cpp:298-309).
+    if (xyz.size() / 3 < 1000) {
+        std::mt19937 rng(1);
+        std::uniform_real_distribution<float> u(-1.0f, 1.0f), u01(0.0f, 1.0f);
+        const float r = float(extent) * 0.6f;
+        for (int k = 0; k < 10000; ++k) {
+            xyz.insert(xyz.end(), {u(rng) * r, u(rng) * r, u(rng) * r});
+            rgb.insert(rgb.end(), {u01(rng), u01(rng), u01(rng)});
+        }
+        say("Few sparse points: added random initial points");
+    }
+    // Training cameras: each full-resolution camera scaled to its training image (Reconstructor.cpp:311-316).
+    std::vector<TrainImage> views(train.size());
+    for (std::size_t k = 0; k < train.size(); ++k) {
+        Cam c = cameras[k].scaled(double(train[k].camera.width) / double(fullWidth[k]));
+        c.width = train[k].camera.width;
+        c.height = train[k].camera.height;
+        train[k].camera = std::decay_t<decltype(train[k].camera)>::fromCamera(c);
+        views[k] = imageFrom(train[k]);
+    }
+    // Train (Reconstructor.cpp:318-345).
+    const GaussianModel init = initGaussiansFromPoints(xyz, rgb);
+    TrainOptions topt = TrainOptions::forIterations(iterations);
+    topt.max_gaussians = maxGaussians;
+    say(format("Training %.0f iterations at %.0f px from %.0f Gaussians (scene extent %.3f)", iterations,
+               double(views[0].camera.width > views[0].camera.height ? views[0].camera.width : views[0].camera.height),
+               double(init.size()), extent));
+    Trainer trainer(init, std::move(views), float(extent), topt);
+    const auto begin = std::chrono::steady_clock::now();
+    while (!trainer.done()) {
+        if (cancelled())
+            return fail("Cancelled");
+        trainer.step();
+        const TrainStats &st = trainer.stats();
+        if (st.iteration % 10 == 0 || trainer.done()) {
+            const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+            const double eta = elapsed / st.iteration * (iterations - st.iteration);
+            report("training", trainStart + (0.98 - trainStart) * st.iteration / double(iterations),
+                   format("Training %.0f / %.0f - %.1f dB - ", st.iteration, iterations, st.psnr) +
+                       format("%.0f Gaussians - %.0f s left", double(st.gaussians), eta));
+        }
+        if (st.iteration % 250 == 0)
+            say(format("iter %5.0f  loss %.4f  psnr %.2f dB  gaussians %.0f", st.iteration, st.loss, st.psnr,
+                       double(st.gaussians)));
+    }
+    // Export (Reconstructor.cpp:347-356): the splat PLY straight from the GPU model.
+    report("export", 0.98, "Saving result");
+    if (u3dg_trainer_write_splat_ply(trainer.handle(), splatPath.c_str()) != U3DG_OK)
+        return fail(u3dg_last_error());
+    result.splatPath = splatPath;
+    result.gaussians = trainer.model().size();
+    result.psnr = trainer.evaluatePsnr();
+    result.extent = extent;
+    return true;
 }
 
 // ------------------------------------------------------------------ learned warm-start (no reference counterpart)
