@@ -363,6 +363,32 @@ int u3dg_adam_reset_opacity_moments(u3dg_adam *adam);
 int u3dg_adam_moments(u3dg_adam *adam, u3dg_model *m, u3dg_model *v);
 void u3dg_adam_destroy(u3dg_adam *adam);
 
+/* ------------------------------------------------------------------ crop (engine/include/u3d/splat/Crop.h) */
+
+/* CropBox (Crop.h:9-19): an axis-aligned box in model coordinates. */
+typedef struct u3dg_crop_box {
+    float min[3], max[3];
+} u3dg_crop_box;
+/* cropModel (Crop.h:21-23, engine/src/splat/Crop.cpp:44-52) on the GPU: keeps the Gaussians whose
+ * centre lies inside box (bounds included) and whose sigmoid(opacity) is at least min_opacity, in
+ * order. Call with out == NULL to get *count first; capacity is out's size. */
+int u3dg_crop_model(const u3dg_model *model, const u3dg_crop_box *box, float min_opacity, u3dg_model *out,
+                    size_t capacity, size_t *count);
+/* suggestCropBox (Crop.h:25-31, Crop.cpp:54-57) on the GPU: per axis, the low / high quantiles of the
+ * centres of Gaussians at least 0.3 opaque (all centres when none is), widened by margin of the
+ * box size (at least 1e-4) on each side. */
+int u3dg_suggest_crop_box(const u3dg_model *model, float low_fraction, float high_fraction, float margin,
+                          u3dg_crop_box *out);
+/* modelBounds (Crop.h:33-35, Crop.cpp:59-62): the 0.5 % / 99.5 % quantiles of all centres plus 10 %. */
+int u3dg_model_bounds(const u3dg_model *model, u3dg_crop_box *out);
+/* No reference counterpart (cropModel applied to the trainer's model where it lives): crops the
+ * trainer's model on the GPU, with its Adam moments, without a round trip through the host; training
+ * may continue afterwards (densification statistics restart at zero). */
+int u3dg_trainer_crop(u3dg_trainer *trainer, const u3dg_crop_box *box, float min_opacity);
+/* suggestCropBox / modelBounds of the trainer's model (low_fraction < 0: modelBounds). */
+int u3dg_trainer_suggest_crop_box(u3dg_trainer *trainer, float low_fraction, float high_fraction, float margin,
+                                  u3dg_crop_box *out);
+
 /* ------------------------------------------------------------------ model I/O and init (host) */
 
 /* initGaussiansFromPoints (engine/include/u3d/splat/GaussianModel.h:41,

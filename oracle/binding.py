@@ -70,10 +70,31 @@ class _Lib:
         _sig(lib, p + "trainer_destroy", None, _P)
         _sig(lib, p + "init_from_points", None, _F, _F, C.c_size_t, _MV)
         _sig(lib, p + "options_for_iterations", None, C.c_int, _OPT)
+        _sig(lib, p + "crop_model", C.c_size_t, _MV, C.POINTER(_abi.CropBox), C.c_float, _MV)
         self.p = p
+
+    def crop_model(self, model: GaussianModel, box, min_opacity: float = 0.0) -> GaussianModel:
+        """cropModel (Crop.cpp:44-52); box = (min xyz, max xyz)."""
+        mv, cb = model.view(), _crop_box(box)
+        n = int(self.fn("crop_model")(C.byref(mv), C.byref(cb), float(min_opacity), None))
+        out = GaussianModel.zeros(n)
+        ov = out.view()
+        self.fn("crop_model")(C.byref(mv), C.byref(cb), float(min_opacity), C.byref(ov))
+        return out
 
     def fn(self, name):
         return getattr(self.lib, self.p + name)
+
+
+def _crop_box(b) -> _abi.CropBox:
+    out = _abi.CropBox()
+    for k in range(3):
+        out.min[k], out.max[k] = float(b[0][k]), float(b[1][k])
+    return out
+
+
+def _unbox(b: _abi.CropBox):
+    return np.array(list(b.min), np.float32), np.array(list(b.max), np.float32)
 
 
 class Raster:
@@ -153,6 +174,19 @@ class Oracle(_Lib):
              C.POINTER(C.c_size_t), _I)
         _sig(lib, "orc_trainer_iteration", C.c_int, _P)
         _sig(lib, "orc_trainer_view_log", C.c_int, _P, _I, C.c_int)
+        _sig(lib, "orc_crop_box", None, _MV, C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(_abi.CropBox))
+
+    def suggest_crop_box(self, model: GaussianModel, lo=0.05, hi=0.95, margin=0.1):
+        """suggestCropBox (Crop.cpp:54-57): quantileBox with an opacity floor of 0.3."""
+        mv, out = model.view(), _abi.CropBox()
+        self.lib.orc_crop_box(C.byref(mv), lo, hi, margin, 0.3, C.byref(out))
+        return _unbox(out)
+
+    def model_bounds(self, model: GaussianModel):
+        """modelBounds (Crop.cpp:59-62)."""
+        mv, out = model.view(), _abi.CropBox()
+        self.lib.orc_crop_box(C.byref(mv), 0.005, 0.995, 0.1, 0.0, C.byref(out))
+        return _unbox(out)
 
     # -- rasterizer
     def raster(self, threads: int = os.cpu_count() or 1) -> "OracleRaster":
@@ -318,6 +352,17 @@ class Reference(_Lib):
         _sig(lib, "ref_pool_threads", C.c_int, C.c_int)
         _sig(lib, "ref_write_splat_ply", C.c_int, C.c_char_p, _MV)
         _sig(lib, "ref_read_splat_ply", C.c_int, C.c_char_p, _MV, C.POINTER(C.c_size_t), C.POINTER(C.c_int))
+        _sig(lib, "ref_crop_box", None, _MV, C.c_float, C.c_float, C.c_float, C.c_int, C.POINTER(_abi.CropBox))
+
+    def suggest_crop_box(self, model: GaussianModel, lo=0.05, hi=0.95, margin=0.1):
+        mv, out = model.view(), _abi.CropBox()
+        self.lib.ref_crop_box(C.byref(mv), lo, hi, margin, 0, C.byref(out))
+        return _unbox(out)
+
+    def model_bounds(self, model: GaussianModel):
+        mv, out = model.view(), _abi.CropBox()
+        self.lib.ref_crop_box(C.byref(mv), 0.0, 0.0, 0.0, 1, C.byref(out))
+        return _unbox(out)
 
     @staticmethod
     def available() -> bool:

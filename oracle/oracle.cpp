@@ -1299,6 +1299,60 @@ int orc_trainer_view_log(Trainer *t, int *out, int capacity)
     return n;
 }
 
+// cropModel (engine/src/splat/Crop.cpp:44-52): centre inside the box and sigmoid(opacity) >= floor.
+size_t orc_crop_model(const u3dg_model *model, const u3dg_crop_box *box, float min_opacity, u3dg_model *out)
+{
+    const orc::Model m = orc::fromView(*model);
+    size_t kept = 0;
+    for (size_t i = 0; i < m.size(); ++i) {
+        const float *p = &m.means[i * 3];
+        const bool in = p[0] >= box->min[0] && p[0] <= box->max[0] && p[1] >= box->min[1] && p[1] <= box->max[1] &&
+                        p[2] >= box->min[2] && p[2] <= box->max[2];
+        if (!in || !(orc::sigmoidf(m.opac[i]) >= min_opacity))
+            continue;
+        if (out) {
+            std::copy(&m.means[i * 3], &m.means[i * 3] + 3, out->means + kept * 3);
+            std::copy(&m.scales[i * 3], &m.scales[i * 3] + 3, out->scales + kept * 3);
+            std::copy(&m.quats[i * 4], &m.quats[i * 4] + 4, out->quats + kept * 4);
+            out->opacities[kept] = m.opac[i];
+            std::copy(&m.colors[i * 3], &m.colors[i * 3] + 3, out->colors + kept * 3);
+        }
+        ++kept;
+    }
+    return kept;
+}
+
+// quantileBox (Crop.cpp:12-40): per axis, the lo / hi quantiles (std::nth_element) of the centres of
+// Gaussians at least min_opacity opaque (all centres when none is), widened by margin (at least 1e-4).
+void orc_crop_box(const u3dg_model *model, float lo, float hi, float margin, float min_opacity, u3dg_crop_box *box)
+{
+    const orc::Model m = orc::fromView(*model);
+    std::vector<float> axis;
+    for (int k = 0; k < 3; ++k) {
+        axis.clear();
+        for (size_t i = 0; i < m.size(); ++i)
+            if (orc::sigmoidf(m.opac[i]) >= min_opacity)
+                axis.push_back(m.means[i * 3 + size_t(k)]);
+        if (axis.empty())
+            for (size_t i = 0; i < m.size(); ++i)
+                axis.push_back(m.means[i * 3 + size_t(k)]);
+        if (axis.empty()) {
+            box->min[k] = -1.0f;
+            box->max[k] = 1.0f;
+            continue;
+        }
+        auto at = [&](float q) {
+            const size_t idx = std::min(axis.size() - 1, size_t(q * float(axis.size() - 1) + 0.5f));
+            std::nth_element(axis.begin(), axis.begin() + std::ptrdiff_t(idx), axis.end());
+            return axis[idx];
+        };
+        const float a = at(lo), b = at(hi);
+        const float pad = std::max((b - a) * margin, 1e-4f);
+        box->min[k] = a - pad;
+        box->max[k] = b + pad;
+    }
+}
+
 void orc_init_from_points(const float *xyz, const float *rgb, size_t n, u3dg_model *out)
 {
     Model m = initFromPoints(xyz, rgb, n);

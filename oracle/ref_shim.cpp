@@ -12,6 +12,7 @@
 
 #include "u3d/ThreadPool.h"
 #include "u3d/splat/Adam.h"
+#include "u3d/splat/Crop.h"
 #include "u3d/splat/GaussianModel.h"
 #include "u3d/splat/Loss.h"
 #include "u3d/splat/Rasterizer.h"
@@ -294,6 +295,28 @@ int ref_read_splat_ply(const char *path, u3dg_model *out, size_t *count, int *is
     if (out)
         fromModel(g, *out);
     return 1;
+}
+
+size_t ref_crop_model(const u3dg_model *model, const u3dg_crop_box *box, float min_opacity, u3dg_model *out)
+{
+    CropBox b;
+    for (int k = 0; k < 3; ++k) {
+        b.min[k] = box->min[k];
+        b.max[k] = box->max[k];
+    }
+    const GaussianModel g = cropModel(toModel(*model), b, min_opacity);
+    if (out)
+        fromModel(g, *out);
+    return g.size();
+}
+
+void ref_crop_box(const u3dg_model *model, float lo, float hi, float margin, int bounds, u3dg_crop_box *box)
+{
+    const CropBox b = bounds ? modelBounds(toModel(*model)) : suggestCropBox(toModel(*model), lo, hi, margin);
+    for (int k = 0; k < 3; ++k) {
+        box->min[k] = b.min[k];
+        box->max[k] = b.max[k];
+    }
 }
 
 } // extern "C"

@@ -636,6 +636,54 @@ def test_forward_on_8x8_blocks_is_bit_exact(u3dg, tiny_scene, tile, depth):
         np.testing.assert_array_equal(out[0], out[1])
 
 
+def test_crop_matches_oracle(u3dg, oracle, tiny_scene):
+    """cropModel / suggestCropBox / modelBounds (Crop.cpp:12-62) on the GPU against the oracle (pinned
+    to the reference): host models with floaters, an all-faint model and an empty one, bit for bit;
+    then the trainer's own model cropped in place, with training continuing afterwards."""
+    rng = np.random.default_rng(32)
+    models = []
+    for n in (20000, 333):
+        means = rng.normal(size=(n, 3)).astype(np.float32)
+        means[: n // 40] *= 25.0
+        models.append(GaussianModel(means, rng.normal(-4, 1, (n, 3)).astype(np.float32),
+                                    rng.normal(size=(n, 4)).astype(np.float32),
+                                    rng.normal(-0.5, 2.0, n).astype(np.float32), rng.normal(size=(n, 3)).astype(np.float32)))
+    faint = models[1].copy()
+    faint.opacities[:] = -9.0
+    models += [faint, GaussianModel.zeros(0)]
+    for m in models:
+        for args in ((0.05, 0.95, 0.1), (0.2, 0.6, 0.5)):
+            g, o = u3dg.suggestCropBox(m, *args), oracle.suggest_crop_box(m, *args)
+            np.testing.assert_array_equal(g[0], o[0])
+            np.testing.assert_array_equal(g[1], o[1])
+        g, o = u3dg.modelBounds(m), oracle.model_bounds(m)
+        np.testing.assert_array_equal(g[0], o[0])
+        np.testing.assert_array_equal(g[1], o[1])
+        box = oracle.suggest_crop_box(m)
+        for floor in (0.0, 0.3):
+            gc, oc = u3dg.cropModel(m, box, floor), oracle.crop_model(m, box, floor)
+            assert gc.size() == oc.size()
+            for name in GROUPS:
+                np.testing.assert_array_equal(getattr(gc, name), getattr(oc, name))
+    sc = tiny_scene
+    t = u3dg.Trainer(oracle.init_from_points(sc.init_xyz, sc.init_rgb), sc.images, sc.extent, sc.options())
+    t.step(100)
+    before = t.model()
+    box = t.suggestCropBox(0.1, 0.9, 0.05)
+    ob = oracle.suggest_crop_box(before, 0.1, 0.9, 0.05)
+    np.testing.assert_array_equal(box[0], ob[0])
+    np.testing.assert_array_equal(box[1], ob[1])
+    bounds = t.suggestCropBox(-1.0)
+    np.testing.assert_array_equal(bounds[0], oracle.model_bounds(before)[0])
+    t.crop(box, 0.05)
+    after, want = t.model(), oracle.crop_model(before, box, 0.05)
+    assert 0 < after.size() < before.size()
+    for name in GROUPS:
+        np.testing.assert_array_equal(getattr(after, name), getattr(want, name))
+    t.step(50)
+    assert t.iteration() == 150 and np.isfinite(t.model().means).all()
+
+
 def test_trainer_writes_the_reference_ply(u3dg, oracle, reference, tiny_scene, tmp_path):
     """The trainer's one-call PLY export writes the same bytes as downloading the model and writing it
     with this library's writer or with the reference's (SplatPly.cpp:261-282)."""

@@ -141,3 +141,35 @@ def test_closed_form_projection_oracle(oracle):
     ys, xs = np.mgrid[0:201, 0:201]
     wsum = v.sum()
     assert abs((v * xs).sum() / wsum - 100) < 0.01 and abs((v * ys).sum() / wsum - 100) < 0.01
+
+
+def _crop_models():
+    rng = np.random.default_rng(31)
+    out = []
+    for n, spread in ((5000, 1.0), (777, 3.0), (1, 1.0)):
+        means = (rng.normal(size=(n, 3)) * spread).astype(np.float32)
+        means[: n // 50] *= 20.0  # far floaters
+        m = GaussianModel(means, rng.normal(-4, 1, (n, 3)).astype(np.float32), rng.normal(size=(n, 4)).astype(np.float32),
+                          rng.normal(-0.5, 2.0, n).astype(np.float32), rng.normal(size=(n, 3)).astype(np.float32))
+        out.append(m)
+    faint = out[1].copy()
+    faint.opacities[:] = -9.0  # nothing 0.3 opaque: the boxes fall back to all centres
+    out.append(faint)
+    out.append(GaussianModel.zeros(0))
+    return out
+
+
+def test_crop_matches_reference(oracle, reference):
+    """cropModel, suggestCropBox and modelBounds (Crop.cpp:12-62): the oracle's restatement against the
+    reference, bit for bit, on models with floaters, an all-faint model, one Gaussian and none."""
+    for m in _crop_models():
+        for lo, hi, margin in ((0.05, 0.95, 0.1), (0.0, 1.0, 0.0), (0.2, 0.6, 0.5)):
+            a, b = oracle.suggest_crop_box(m, lo, hi, margin), reference.suggest_crop_box(m, lo, hi, margin)
+            np.testing.assert_array_equal(a[0], b[0])
+            np.testing.assert_array_equal(a[1], b[1])
+        a, b = oracle.model_bounds(m), reference.model_bounds(m)
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
+        box = oracle.suggest_crop_box(m)
+        for floor in (0.0, 0.3, 0.7):
+            _equal_models(oracle.crop_model(m, box, floor), reference.crop_model(m, box, floor))

@@ -52,6 +52,12 @@ class RasterSettings(C.Structure):
     ]
 
 
+class CropBox(C.Structure):
+    """u3dg_crop_box == CropBox (engine/include/u3d/splat/Crop.h:9-19)."""
+
+    _fields_ = [("min", C.c_float * 3), ("max", C.c_float * 3)]
+
+
 class LearningRates(C.Structure):
     """u3dg_learning_rates == LearningRates (engine/include/u3d/splat/Adam.h:8-14)."""
 

@@ -51,6 +51,17 @@ class Trainer:
         # The pixel arrays the C side reads (contiguous copies where needed) live as long as the trainer.
         self._keep = keep if background_upload else None
 
+    def crop(self, box, min_opacity: float = 0.0) -> None:
+        """cropModel of the trainer's model on the GPU (with its Adam moments); box = (min, max)."""
+        cb = _box(box)
+        check(load().u3dg_trainer_crop(self._h, C.byref(cb), float(min_opacity)))
+
+    def suggestCropBox(self, low_fraction: float = 0.05, high_fraction: float = 0.95, margin: float = 0.1):
+        """suggestCropBox of the trainer's model (low_fraction < 0: modelBounds)."""
+        out = _abi.CropBox()
+        check(load().u3dg_trainer_suggest_crop_box(self._h, low_fraction, high_fraction, margin, C.byref(out)))
+        return _unbox(out)
+
     def wait_uploads(self) -> None:
         """Blocks until every training image is on the GPU (background upload)."""
         check(load().u3dg_trainer_wait_uploads(self._h))
@@ -465,6 +476,45 @@ def readSplatPly(path: str, result: PlyResult | None = None):
     v = m.view()
     check(L.u3dg_read_splat_ply(str(path).encode(), C.byref(v), n.value, C.byref(n), C.byref(is_splat)))
     return m, bool(is_splat.value)
+
+
+def _box(b) -> _abi.CropBox:
+    if isinstance(b, _abi.CropBox):
+        return b
+    lo, hi = b
+    out = _abi.CropBox()
+    for k in range(3):
+        out.min[k], out.max[k] = float(lo[k]), float(hi[k])
+    return out
+
+
+def _unbox(b: _abi.CropBox):
+    return np.array(list(b.min), np.float32), np.array(list(b.max), np.float32)
+
+
+def cropModel(model: GaussianModel, box, min_opacity: float = 0.0) -> GaussianModel:
+    """cropModel (Crop.h:21-23) on the GPU; box = (min xyz, max xyz)."""
+    mv, cb, n = model.view(), _box(box), C.c_size_t()
+    check(load().u3dg_crop_model(C.byref(mv), C.byref(cb), float(min_opacity), None, 0, C.byref(n)))
+    out = GaussianModel.zeros(n.value)
+    ov = out.view()
+    check(load().u3dg_crop_model(C.byref(mv), C.byref(cb), float(min_opacity), C.byref(ov), n.value, C.byref(n)))
+    return out
+
+
+def suggestCropBox(model: GaussianModel, low_fraction: float = 0.05, high_fraction: float = 0.95,
+                   margin: float = 0.1):
+    """suggestCropBox (Crop.h:25-31) on the GPU: (min xyz, max xyz)."""
+    mv, out = model.view(), _abi.CropBox()
+    check(load().u3dg_suggest_crop_box(C.byref(mv), low_fraction, high_fraction, margin, C.byref(out)))
+    return _unbox(out)
+
+
+def modelBounds(model: GaussianModel):
+    """modelBounds (Crop.h:33-35) on the GPU: (min xyz, max xyz)."""
+    mv, out = model.view(), _abi.CropBox()
+    check(load().u3dg_model_bounds(C.byref(mv), C.byref(out)))
+    return _unbox(out)
 
 
 def renderSh(model: GaussianModel, sh_rest: np.ndarray | None, degree: int, camera,

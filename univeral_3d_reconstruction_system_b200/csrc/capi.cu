@@ -1058,6 +1058,95 @@ int u3dg_init_gaussians_from_points(const float *xyz, const float *rgb, size_t n
     });
 }
 
+// ------------------------------------------------------------------ crop
+
+static void requireBox(const u3dg_crop_box *box)
+{
+    if (!box)
+        throw StatusError(U3DG_ERR_INVALID_ARG, "crop box is NULL");
+}
+
+int u3dg_crop_model(const u3dg_model *model, const u3dg_crop_box *box, float min_opacity, u3dg_model *out,
+                    size_t capacity, size_t *count)
+{
+    return guarded([&] {
+        requireModel(model, "model");
+        requireBox(box);
+        if (!count)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "count is NULL");
+        requireDevice();
+        Stream st;
+        DevModel in;
+        in.upload(*model, st.s);
+        const int n = int(model->count);
+        DevBuf<int> keep, pos, scratch;
+        const size_t kept = cropKeep(in.params(), n, *box, min_opacity, keep, pos, scratch, st.s);
+        *count = kept;
+        if (!out)
+            return;
+        if (kept > capacity)
+            throw StatusError(U3DG_ERR_CAPACITY, "output capacity too small");
+        requireModel(out, "out");
+        DevModel res;
+        res.cap = std::max<size_t>(kept, 1);
+        res.buf.reserve(14 * res.cap, true);
+        launchCropWrite(in.buf.p, in.cap, res.buf.p, res.cap, 1, n, keep.p, pos.p, st.s);
+        U3DG_CUDA(cudaGetLastError());
+        res.download(*out, kept, st.s);
+        st.sync();
+    });
+}
+
+int u3dg_suggest_crop_box(const u3dg_model *model, float low_fraction, float high_fraction, float margin,
+                          u3dg_crop_box *out)
+{
+    return guarded([&] {
+        requireModel(model, "model");
+        requireBox(out);
+        requireDevice();
+        Stream st;
+        DevModel in;
+        in.upload(*model, st.s);
+        // suggestCropBox weighs towards opaque Gaussians: opacity floor 0.3 (Crop.cpp:54-57).
+        *out = quantileBoxOnDevice(in.params(), int(model->count), low_fraction, high_fraction, margin, 0.3f, st.s);
+    });
+}
+
+int u3dg_model_bounds(const u3dg_model *model, u3dg_crop_box *out)
+{
+    return guarded([&] {
+        requireModel(model, "model");
+        requireBox(out);
+        requireDevice();
+        Stream st;
+        DevModel in;
+        in.upload(*model, st.s);
+        *out = quantileBoxOnDevice(in.params(), int(model->count), 0.005f, 0.995f, 0.1f, 0.0f, st.s); // Crop.cpp:59-62
+    });
+}
+
+int u3dg_trainer_crop(u3dg_trainer *trainer, const u3dg_crop_box *box, float min_opacity)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        requireBox(box);
+        t.crop(*box, min_opacity);
+    });
+}
+
+int u3dg_trainer_suggest_crop_box(u3dg_trainer *trainer, float low_fraction, float high_fraction, float margin,
+                                  u3dg_crop_box *out)
+{
+    return guarded([&] {
+        TrainerImpl &t = impl(trainer);
+        requireBox(out);
+        t.finish();
+        *out = low_fraction < 0.0f
+                   ? quantileBoxOnDevice(t.params(), t.n, 0.005f, 0.995f, 0.1f, 0.0f, t.stream)
+                   : quantileBoxOnDevice(t.params(), t.n, low_fraction, high_fraction, margin, 0.3f, t.stream);
+    });
+}
+
 int u3dg_write_splat_ply(const char *path, const u3dg_model *model)
 {
     return guarded([&] {

@@ -1225,6 +1225,21 @@ void TrainerImpl::densifyAndPrune()
         ws.reserveIntersections(16 * size_t(n));
 }
 
+void TrainerImpl::crop(const u3dg_crop_box &box, float minOpacity)
+{
+    finish();
+    const int other = 1 - cur;
+    const size_t kept = cropKeep(params(), n, box, minOpacity, keep, keepScan, dScanPartial, stream);
+    // Parameters and both moments (three consecutive arenas) into the other arena set, then flip.
+    launchCropWrite(arena[cur].p, cap, arena[other].p, cap, 3, n, keep.p, keepScan.p, stream);
+    U3DG_CUDA(cudaGetLastError());
+    cur = other;
+    n = int(kept);
+    U3DG_CUDA(cudaMemsetAsync(gradAccum.p, 0, size_t(std::max(n, 1)) * sizeof(float), stream));
+    U3DG_CUDA(cudaMemsetAsync(gradCount.p, 0, size_t(std::max(n, 1)) * sizeof(int), stream));
+    sync();
+}
+
 void TrainerImpl::resetOpacity()
 {
     // logit(0.01f) in host float arithmetic (GaussianModel.h:13, Trainer.cpp:173).

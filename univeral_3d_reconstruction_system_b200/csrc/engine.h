@@ -389,6 +389,8 @@ struct TrainerImpl {
     void finish();
     void densifyAndPrune();
     void resetOpacity();
+    // cropModel (Crop.cpp:44-52) of the live model with its Adam moments; statistics restart at zero.
+    void crop(const u3dg_crop_box &box, float minOpacity);
     float evaluatePsnr();
     void render(const u3dg_camera &c, float *hostRgb);
     void download(u3dg_model &out);
@@ -443,6 +445,17 @@ private:
     // Checks the oldest queued step; returns false (after rolling back) when it had overflowed.
     bool checkOldest();
 };
+
+// crop.cu: cropModel / suggestCropBox / modelBounds (Crop.cpp:12-62) on device arrays. cropKeep fills
+// keep[i] and its exclusive scan pos (n + 1 entries) and returns the kept count (waits for the stream);
+// launchCropWrite copies the kept rows of `arenas` consecutive 14-float arenas; quantileBoxOnDevice is
+// quantileBox (Crop.cpp:12-40) with the per-axis quantiles taken by a device sort.
+size_t cropKeep(const Params &P, int n, const u3dg_crop_box &box, float minOpacity, DevBuf<int> &keep,
+                DevBuf<int> &pos, DevBuf<int> &scratch, cudaStream_t s);
+void launchCropWrite(const float *src, size_t srcCap, float *dst, size_t dstCap, int arenas, int n, const int *keep,
+                     const int *pos, cudaStream_t s);
+u3dg_crop_box quantileBoxOnDevice(const Params &P, int n, float lo, float hi, float margin, float minOpacity,
+                                  cudaStream_t s);
 
 // Densification on device arrays (shared by the trainer and the unit entry point).
 struct DensifyResult {
