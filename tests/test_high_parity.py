@@ -7,7 +7,8 @@ backward. Checked per step, as one training step computes them:
   - tile lists and their depth order: bit-exact against binTiles on identical projected records
     (the 300k depth sort and ~2.5M intersections), and with culling on, every tile's list is an
     order-preserving subsequence of the reference's list for that tile;
-  - image within 1e-5 absolute per channel, final transmittance within 1e-5, contributor counts exact;
+  - image within 1e-5 absolute per channel, final transmittance within 1e-5, contributor counts exact
+    (with culling, a count indexes the culled list: it must name the same last contributor);
   - per-parameter gradients of the L1 + 0.2 D-SSIM loss against the view's target within 1e-4
     relative (floor: 1% of the group's largest magnitude) and the NDC densification statistic.
 Models: the bench workload (initGaussiansFromPoints of every true centre plus 50k re-samples:
@@ -48,7 +49,8 @@ def model(request, high, oracle):
 
 
 def _subsequence_lists(off, lst, roff, rlst, n):
-    """Every tile's list in (off, lst) is an order-preserving subsequence of its list in (roff, rlst)."""
+    """Every tile's list in (off, lst) is an order-preserving subsequence of its list in (roff, rlst);
+    returns the position in rlst of every entry of lst."""
     tiles = len(roff) - 1
     rt = np.repeat(np.arange(tiles, dtype=np.int64), np.diff(roff))
     rkey = rt * n + rlst.astype(np.int64)  # unique per (tile, Gaussian), increasing position in rlst
@@ -61,6 +63,20 @@ def _subsequence_lists(off, lst, roff, rlst, n):
     pos = order[idx]  # position of each culled entry in the reference list
     same_tile = t[1:] == t[:-1]
     assert np.all(pos[1:][same_tile] > pos[:-1][same_tile]), "culled lists changed the depth order"
+    return pos
+
+
+def _culled_counts_as_reference(nc, off, pos, roff, width, height, tile=16):
+    """Contributor counts over culled lists (an index into the pixel's tile's culled list) expressed as
+    counts over the reference's lists: the last contributor's position in the reference list + 1."""
+    ys, xs = np.mgrid[0:height, 0:width]
+    t = ((ys // tile) * ((width + tile - 1) // tile) + xs // tile).reshape(-1)
+    nc = nc.reshape(-1).astype(np.int64)
+    last = off[t].astype(np.int64) + nc - 1  # global index of the last contributor in lst
+    out = np.zeros_like(nc)
+    has = nc > 0
+    out[has] = pos[last[has]] - roff[t[has]] + 1
+    return out
 
 
 def test_high_step_matches_oracle(u3dg, oracle, high, model):
@@ -86,11 +102,12 @@ def test_high_step_matches_oracle(u3dg, oracle, high, model):
     img = r.forward(model, cam, st)
     assert float(np.max(np.abs(img - ref_img))) <= 1e-5
     ft, nc = r.pixel_state()
-    np.testing.assert_array_equal(nc, ref_nc)
     assert float(np.max(np.abs(ft - ref_ft))) <= 1e-5
     off, lst = r.tiles()
     assert len(lst) < len(ref_list)
-    _subsequence_lists(off, lst, ref_off, ref_list, n)
+    pos = _subsequence_lists(off, lst, ref_off, ref_list, n)
+    # A pixel's contributor count indexes its tile's (culled) list: the same last contributor.
+    np.testing.assert_array_equal(_culled_counts_as_reference(nc, off, pos, ref_off, cam.width, cam.height), ref_nc)
 
     # The step's loss gradient (oracle's loss on the oracle's image), through both backward passes.
     _, dl = oracle.photometric_loss(ref_img, target, cam.width, cam.height, 0.2)
@@ -104,10 +121,13 @@ def test_high_step_matches_oracle(u3dg, oracle, high, model):
     ok, worst = grad_close(ndc, ondc, rel=1e-4)
     assert ok, ("ndc", worst)
 
-    # Culling off at the unit boundary: the reference's own lists.
+    # Culling off at the unit boundary: the reference's own lists and contributor counts.
     r.set_tile_culling(False)
     img2 = r.forward(model, cam, st)
     np.testing.assert_array_equal(img2, img)
     off2, lst2 = r.tiles()
     np.testing.assert_array_equal(off2, ref_off)
     np.testing.assert_array_equal(lst2, ref_list)
+    ft2, nc2 = r.pixel_state()
+    np.testing.assert_array_equal(nc2, ref_nc)
+    np.testing.assert_array_equal(ft2, ft)

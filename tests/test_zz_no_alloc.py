@@ -58,7 +58,7 @@ def env():
     return _lib.load(), torch
 
 
-@pytest.mark.parametrize("h,w,lam", [(61, 97, 0.2), (480, 640, 0.2), (800, 1280, 0.2), (33, 40, 0.0)])
+@pytest.mark.parametrize("h,w,lam", [(61, 97, 0.2), (480, 640, 0.2), (33, 40, 0.0)])
 def test_noalloc_matches_allocating_entry_twice(env, h, w, lam):
     lib, torch = env
     render, target = _images(h, w, seed=h * 1000 + w)
@@ -82,7 +82,7 @@ def test_noalloc_on_a_caller_stream(env):
 
 def test_noalloc_rejects_images_beyond_the_scratch(env):
     lib, torch = env
-    for h, w in ((1040, 1024), (1, 65_537), (16, 65_600), (32_784, 32)):  # 2080, 2049, 2050, 2049 blocks
+    for h, w in ((481, 640), (1, 307_201), (1, 307_200), (307_200, 1)):
         buf = torch.zeros(h * w * 3, device="cuda")
         out = _abi.LossValue()
         st = lib.u3dg_photometric_loss_noalloc(buf.data_ptr(), buf.data_ptr(), w, h, 0.2, buf.data_ptr(),

@@ -757,18 +757,19 @@ int u3dg_photometric_loss(const float *render, const float *target, int width, i
         requireDevice();
         Stream st;
         const size_t P = size_t(width) * height;
-        DevBuf<float> dr, dt, dg;
+        DevBuf<float> dr, dt, dg, dabc;
         DevBuf<double> sums;
         DevBuf<float> vals;
         dr.reserve(P * 3, true);
         dt.reserve(P * 3, true);
         dg.reserve(P * 3, true);
+        dabc.reserve(P * 9, true);
         const int blocks = lossBlocks(width, height);
         sums.reserve(size_t(blocks) * 3, true);
         vals.reserve(4, true);
         U3DG_CUDA(cudaMemcpyAsync(dr.p, render, P * 12, cudaMemcpyHostToDevice, st.s));
         U3DG_CUDA(cudaMemcpyAsync(dt.p, target, P * 12, cudaMemcpyHostToDevice, st.s));
-        LossScratch ls{sums.p, blocks};
+        LossScratch ls{dabc.p, sums.p, blocks};
         launchLoss(dr.p, dt.p, nullptr, width, height, lambda, dg.p, ls, st.s);
         launchLossFinalize(ls, width, height, lambda, nullptr, 0, nullptr, vals.p, vals.p + 3, st.s);
         U3DG_CUDA(cudaGetLastError());

@@ -349,6 +349,7 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
         }
     }
     dLoss.reserve(maxP * 3);
+    abc.reserve(maxP * 9);
     dStats.reserve(1, true);
     hStats.reserve(1);
     U3DG_CUDA(cudaMemsetAsync(dStats.p, 0, sizeof(DevStats), stream));
@@ -661,7 +662,7 @@ void TrainerImpl::launchStep(const StepValues &sv, const StepDesc *desc, BinCoun
     // Loss (Trainer.cpp:67-71) and the step's stats (Trainer.cpp:88-92).
     const int lb = lossBlocks(W, H);
     lossBlockSums.reserve(size_t(lb) * 3);
-    LossScratch ls{lossBlockSums.p, lb};
+    LossScratch ls{abc.p, lossBlockSums.p, lb};
     launchLoss(ws.rgb.p, nullptr, sv.d.target, W, H, o.ssim_lambda, dLoss.p, ls, stream, desc);
     launchLossFinalize(ls, W, H, o.ssim_lambda, dStats.p, sv.d.iteration + 1, ws.counts.p, nullptr, nullptr, stream,
                        desc);

@@ -313,7 +313,7 @@ struct TrainerImpl {
     std::vector<size_t> imageOffset;
     DevBuf<uint8_t> images;
     RasterWorkspace ws;
-    DevBuf<float> dLoss;
+    DevBuf<float> dLoss, abc;
     DevBuf<double> lossBlockSums, psnrSums;
     DevBuf<DevStats> dStats;
     HostPinned<DevStats> hStats;

@@ -164,6 +164,7 @@ void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const flo
 
 // loss.cu
 struct LossScratch {
+    float *abc;        // 3 maps x 3 channels x P
     double *blockSums; // 3 doubles per block: l1, ssim, squared error
     int blocks;
 };

@@ -1,11 +1,11 @@
 // loss.cu - (1 - lambda) L1 + lambda (1 - SSIM) and its gradient (photometricLoss, Loss.cpp:47-184).
 //
 // The reference runs four separable passes over (channel, row) pairs with full-image scratch maps.
-// Here one tiled kernel (lossKernel) does all four passes for a 32x16 tile with the blurs staged in
-// shared memory: L1 term, horizontal + vertical blur of x, y, x^2, y^2, xy, SSIM and its three
-// per-pixel partials (passes 1 and 2) over the tile and a 5-pixel halo, then the blur of the partials
-// and the chain rule into dL/drender (passes 3 and 4; the Gaussian blur is self-adjoint), with block
-// partial sums in double.
+// Here two tiled kernels do the same arithmetic with the blurs staged in shared memory:
+//   lossForwardKernel : L1 term + horizontal blur of x, y, x^2, y^2, xy + vertical blur + SSIM and
+//                       its three per-pixel partials (passes 1 and 2), block partial sums in double;
+//   lossBackwardKernel: horizontal + vertical blur of the partials and the chain rule into
+//                       dL/drender (passes 3 and 4; the Gaussian blur is self-adjoint).
 // Zero padding is reproduced by loading zeros outside the image: the reference skips out-of-image
 // taps, and adding w * 0 to the running sums leaves every intermediate value unchanged, so each
 // per-pixel value keeps the reference's rounding (the file is compiled with -fmad=false). The
@@ -21,6 +21,7 @@ namespace {
 
 constexpr int kR = 5;                    // 11x11 window (Loss.cpp:11)
 constexpr int kTW = 32, kTH = 16;        // output tile
+constexpr int kIW = kTW + 2 * kR, kIH = kTH + 2 * kR;
 constexpr int kThreads = 256;
 
 // The 11 blur weights, passed to the loss kernels by value: kernel parameters sit in the constant
@@ -63,36 +64,15 @@ __device__ __forceinline__ double blockSumDouble(double v)
     return t;
 }
 
-// The whole loss of one 32x16 output tile and one channel at a time, in one kernel. The gradient of
-// the D-SSIM term at a pixel needs the three SSIM partials (abc) of the 11x11 window around it, and
-// each of those needs the blurred statistics of the window around that pixel: the tile stages its
-// inputs with a 10-pixel halo, computes the statistics and the partials for the tile plus a 5-pixel
-// halo, and blurs the partials back onto the tile. The halo partials are the ones the neighbouring
-// tiles compute for their own pixels (same inputs, same operations in the same order), so every value
-// is what the two-pass formulation of Loss.cpp:47-184 gives, without the partials' round trip through
-// global memory. The L1 and SSIM sums of a block cover its own pixels only, in a fixed per-thread
-// order.
-constexpr int kH = 2 * kR;                    // input halo: 10 pixels
-constexpr int kSW = kTW + 2 * kH, kSH = kTH + 2 * kH; // staged inputs: 52 x 36
-constexpr int kAW = kTW + 2 * kR, kAH = kTH + 2 * kR; // statistics / partials region: 42 x 26
-
-struct LossSmem {
-    float x[kSH][kSW], y[kSH][kSW];   // render and target of one channel
-    float hm[5][kSH][kAW];           // horizontal blurs of x, y, x^2, y^2, xy (then of the partials)
-    float abc[3][kAH][kAW];          // SSIM partials over the tile and its 5-pixel halo
-    float v[kTH][kTW];               // SSIM of the tile's pixels
-};
-
-__global__ void __launch_bounds__(kThreads) lossKernel(const float *render, const float *targetF,
-                                                       const uint8_t *targetU8, int W, int H, float lambda,
-                                                       float *grad, double *blockSums, const StepDesc *desc,
-                                                       const SsimWindow cWin)
+__global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *render, const float *targetF,
+                                                              const uint8_t *targetU8, int W, int H, float lambda,
+                                                              float *grad, float *abc, double *blockSums,
+                                                              const StepDesc *desc, const SsimWindow cWin)
 {
     if (desc)
         targetU8 = desc->target;
-    extern __shared__ __align__(16) unsigned char lossSmemRaw[];
-    LossSmem &sm = *reinterpret_cast<LossSmem *>(lossSmemRaw);
-    float(*h2)[kAH][kTW] = reinterpret_cast<float(*)[kAH][kTW]>(&sm.hm[0][0][0]); // blurred partials
+    __shared__ float sx[kIH][kIW], sy[kIH][kIW];
+    __shared__ float hm[5][kIH][kTW];
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
     const size_t P = size_t(W) * H;
     const float invCount = 1.0f / float(P * 3);
@@ -101,139 +81,78 @@ __global__ void __launch_bounds__(kThreads) lossKernel(const float *render, cons
     const float kC1 = 0.01f * 0.01f, kC2 = 0.03f * 0.03f;
     const float inv255 = 1.0f / 255.0f;
     double l1 = 0.0, ssim = 0.0, sq = 0.0;
-    constexpr int kPix = kTW * kTH / kThreads; // tile pixels per thread (2)
     for (int c = 0; c < 3; ++c) {
-        for (int k = threadIdx.x; k < kSW * kSH; k += kThreads) {
-            const int ix = k % kSW, iy = k / kSW;
-            const int gx = x0 + ix - kH, gy = y0 + iy - kH;
+        for (int k = threadIdx.x; k < kIW * kIH; k += kThreads) {
+            const int ix = k % kIW, iy = k / kIW;
+            const int gx = x0 + ix - kR, gy = y0 + iy - kR;
             float a = 0.0f, b = 0.0f;
             if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
                 const size_t idx = (size_t(gy) * W + gx) * 3 + c;
                 a = render[idx];
                 b = targetU8 ? float(targetU8[idx]) * inv255 : targetF[idx];
             }
-            sm.x[iy][ix] = a;
-            sm.y[iy][ix] = b;
+            sx[iy][ix] = a;
+            sy[iy][ix] = b;
         }
         __syncthreads();
         // L1 term for this tile's pixels (Loss.cpp:68-74).
-        float l1grad[kPix];
-#pragma unroll
-        for (int r = 0; r < kPix; ++r) {
-            const int k = threadIdx.x + r * kThreads;
+        for (int k = threadIdx.x; k < kTW * kTH; k += kThreads) {
             const int ox = k % kTW, oy = k / kTW;
             const int gx = x0 + ox, gy = y0 + oy;
-            l1grad[r] = 0.0f;
             if (gx < W && gy < H) {
-                const float d = sm.x[oy + kH][ox + kH] - sm.y[oy + kH][ox + kH];
+                const float d = sx[oy + kR][ox + kR] - sy[oy + kR][ox + kR];
                 l1 += fabs(double(d));
-                const double dd = double(sm.x[oy + kH][ox + kH]) - double(sm.y[oy + kH][ox + kH]);
+                const double dd = double(sx[oy + kR][ox + kR]) - double(sy[oy + kR][ox + kR]);
                 sq += dd * dd;
-                l1grad[r] = l1Scale * (d > 0 ? 1.0f : (d < 0 ? -1.0f : 0.0f));
+                grad[(size_t(gy) * W + gx) * 3 + c] = l1Scale * (d > 0 ? 1.0f : (d < 0 ? -1.0f : 0.0f));
             }
         }
         if (lambda > 0.0f) {
-            // Horizontal blur of x, y, x^2, y^2, xy (Loss.cpp:77-94) for every staged row, over the
-            // columns of the tile and its 5-pixel halo.
-            for (int k = threadIdx.x; k < kAW * kSH; k += kThreads) {
-                const int ox = k % kAW, iy = k / kAW;
+            // Horizontal blur of x, y, x^2, y^2, xy (Loss.cpp:77-94).
+            for (int k = threadIdx.x; k < kTW * kIH; k += kThreads) {
+                const int ox = k % kTW, iy = k / kTW;
                 float s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * kR; ++t) {
-                    const float a = sm.x[iy][ox + t], b = sm.y[iy][ox + t], w = cWin.w[t];
+                    const float a = sx[iy][ox + t], b = sy[iy][ox + t], w = cWin.w[t];
                     s0 += w * a;
                     s1 += w * b;
                     s2 += w * a * a;
                     s3 += w * b * b;
                     s4 += w * a * b;
                 }
-                sm.hm[0][iy][ox] = s0;
-                sm.hm[1][iy][ox] = s1;
-                sm.hm[2][iy][ox] = s2;
-                sm.hm[3][iy][ox] = s3;
-                sm.hm[4][iy][ox] = s4;
+                hm[0][iy][ox] = s0;
+                hm[1][iy][ox] = s1;
+                hm[2][iy][ox] = s2;
+                hm[3][iy][ox] = s3;
+                hm[4][iy][ox] = s4;
             }
             __syncthreads();
-            // Vertical blur, SSIM and its partials (Loss.cpp:113-137) over the tile and its halo;
-            // partials outside the image are zero (the blur of pass 3 pads with zeros).
-            for (int k = threadIdx.x; k < kAW * kAH; k += kThreads) {
-                const int ox = k % kAW, oy = k / kAW;
-                const int gx = x0 + ox - kR, gy = y0 + oy - kR;
-                float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-                if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-                    float m[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-                    for (int t = 0; t <= 2 * kR; ++t) {
-                        const float w = cWin.w[t];
-#pragma unroll
-                        for (int j = 0; j < 5; ++j)
-                            m[j] += w * sm.hm[j][oy + t][ox];
-                    }
-                    const float mx = m[0], my = m[1];
-                    const float vx = m[2] - mx * mx, vy = m[3] - my * my, vxy = m[4] - mx * my;
-                    const float A1 = 2 * mx * my + kC1, A2 = 2 * vxy + kC2;
-                    const float B1 = mx * mx + my * my + kC1, B2 = vx + vy + kC2;
-                    const float v = (A1 * A2) / (B1 * B2);
-                    const float dmu = (2 * my * A2 - 2 * my * A1) / (B1 * B2) - v * (2 * mx / B1 - 2 * mx / B2);
-                    a0 = dLds * dmu;
-                    a1 = dLds * (-v / B2);
-                    a2 = dLds * (2 * A1 / (B1 * B2));
-                    if (ox >= kR && ox < kR + kTW && oy >= kR && oy < kR + kTH)
-                        sm.v[oy - kR][ox - kR] = v;
-                }
-                sm.abc[0][oy][ox] = a0;
-                sm.abc[1][oy][ox] = a1;
-                sm.abc[2][oy][ox] = a2;
-            }
-            __syncthreads();
-            // SSIM sum over the tile's own pixels, in the order each thread owns them.
-#pragma unroll
-            for (int r = 0; r < kPix; ++r) {
-                const int k = threadIdx.x + r * kThreads;
+            // Vertical blur, SSIM and its partials (Loss.cpp:113-137).
+            for (int k = threadIdx.x; k < kTW * kTH; k += kThreads) {
                 const int ox = k % kTW, oy = k / kTW;
-                if (x0 + ox < W && y0 + oy < H)
-                    ssim += double(sm.v[oy][ox]);
-            }
-            // Horizontal blur of the partials (pass 3, Loss.cpp:142-157), into the first maps' space.
-            for (int k = threadIdx.x; k < kTW * kAH; k += kThreads) {
-                const int ox = k % kTW, iy = k / kTW;
-                float b0 = 0, b1 = 0, b2 = 0;
+                const int gx = x0 + ox, gy = y0 + oy;
+                if (gx >= W || gy >= H)
+                    continue;
+                float m[5] = {0, 0, 0, 0, 0};
 #pragma unroll
                 for (int t = 0; t <= 2 * kR; ++t) {
                     const float w = cWin.w[t];
-                    b0 += w * sm.abc[0][iy][ox + t];
-                    b1 += w * sm.abc[1][iy][ox + t];
-                    b2 += w * sm.abc[2][iy][ox + t];
-                }
-                h2[0][iy][ox] = b0;
-                h2[1][iy][ox] = b1;
-                h2[2][iy][ox] = b2;
-            }
-            __syncthreads();
-        }
-        // Vertical blur of the partials and the chain rule into dL/drender (pass 4, Loss.cpp:160-177),
-        // added to the L1 term.
 #pragma unroll
-        for (int r = 0; r < kPix; ++r) {
-            const int k = threadIdx.x + r * kThreads;
-            const int ox = k % kTW, oy = k / kTW;
-            const int gx = x0 + ox, gy = y0 + oy;
-            if (gx >= W || gy >= H)
-                continue;
-            const size_t idx = (size_t(gy) * W + gx) * 3 + c;
-            if (lambda > 0.0f) {
-                float g0 = 0, g1 = 0, g2 = 0;
-#pragma unroll
-                for (int t = 0; t <= 2 * kR; ++t) {
-                    const float w = cWin.w[t];
-                    g0 += w * h2[0][oy + t][ox];
-                    g1 += w * h2[1][oy + t][ox];
-                    g2 += w * h2[2][oy + t][ox];
+                    for (int j = 0; j < 5; ++j)
+                        m[j] += w * hm[j][oy + t][ox];
                 }
-                const float rv = sm.x[oy + kH][ox + kH], tg = sm.y[oy + kH][ox + kH];
-                grad[idx] = l1grad[r] + (g0 + 2.0f * rv * g1 + tg * g2);
-            } else {
-                grad[idx] = l1grad[r];
+                const float mx = m[0], my = m[1];
+                const float vx = m[2] - mx * mx, vy = m[3] - my * my, vxy = m[4] - mx * my;
+                const float a1 = 2 * mx * my + kC1, a2 = 2 * vxy + kC2;
+                const float b1 = mx * mx + my * my + kC1, b2 = vx + vy + kC2;
+                const float v = (a1 * a2) / (b1 * b2);
+                ssim += double(v);
+                const float dmu = (2 * my * a2 - 2 * my * a1) / (b1 * b2) - v * (2 * mx / b1 - 2 * mx / b2);
+                const size_t o = size_t(c) * P + size_t(gy) * W + gx;
+                abc[o] = dLds * dmu;
+                abc[3 * P + o] = dLds * (-v / b2);
+                abc[6 * P + o] = dLds * (2 * a1 / (b1 * b2));
             }
         }
         __syncthreads();
@@ -246,6 +165,67 @@ __global__ void __launch_bounds__(kThreads) lossKernel(const float *render, cons
         blockSums[3 * b] = t0;
         blockSums[3 * b + 1] = t1;
         blockSums[3 * b + 2] = t2;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *render, const float *targetF,
+                                                               const uint8_t *targetU8, int W, int H, const float *abc,
+                                                               float *grad, const StepDesc *desc,
+                                                               const SsimWindow cWin)
+{
+    if (desc)
+        targetU8 = desc->target;
+    __shared__ float sm[3][kIH][kIW];
+    __shared__ float hm[3][kIH][kTW];
+    const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
+    const size_t P = size_t(W) * H;
+    const float inv255 = 1.0f / 255.0f;
+    for (int c = 0; c < 3; ++c) {
+        for (int k = threadIdx.x; k < kIW * kIH; k += kThreads) {
+            const int ix = k % kIW, iy = k / kIW;
+            const int gx = x0 + ix - kR, gy = y0 + iy - kR;
+            const bool in = gx >= 0 && gx < W && gy >= 0 && gy < H;
+            const size_t o = size_t(c) * P + (in ? size_t(gy) * W + gx : 0);
+            sm[0][iy][ix] = in ? abc[o] : 0.0f;
+            sm[1][iy][ix] = in ? abc[3 * P + o] : 0.0f;
+            sm[2][iy][ix] = in ? abc[6 * P + o] : 0.0f;
+        }
+        __syncthreads();
+        // Pass 3: horizontal blur of the partials (Loss.cpp:142-157).
+        for (int k = threadIdx.x; k < kTW * kIH; k += kThreads) {
+            const int ox = k % kTW, iy = k / kTW;
+            float a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+            for (int t = 0; t <= 2 * kR; ++t) {
+                const float w = cWin.w[t];
+                a0 += w * sm[0][iy][ox + t];
+                a1 += w * sm[1][iy][ox + t];
+                a2 += w * sm[2][iy][ox + t];
+            }
+            hm[0][iy][ox] = a0;
+            hm[1][iy][ox] = a1;
+            hm[2][iy][ox] = a2;
+        }
+        __syncthreads();
+        // Pass 4: vertical blur + chain rule (Loss.cpp:160-177).
+        for (int k = threadIdx.x; k < kTW * kTH; k += kThreads) {
+            const int ox = k % kTW, oy = k / kTW;
+            const int gx = x0 + ox, gy = y0 + oy;
+            if (gx >= W || gy >= H)
+                continue;
+            float g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+            for (int t = 0; t <= 2 * kR; ++t) {
+                const float w = cWin.w[t];
+                g0 += w * hm[0][oy + t][ox];
+                g1 += w * hm[1][oy + t][ox];
+                g2 += w * hm[2][oy + t][ox];
+            }
+            const size_t idx = (size_t(gy) * W + gx) * 3 + c;
+            const float tg = targetU8 ? float(targetU8[idx]) * inv255 : targetF[idx];
+            grad[idx] += g0 + 2.0f * render[idx] * g1 + tg * g2;
+        }
+        __syncthreads();
     }
 }
 
@@ -355,14 +335,11 @@ void launchLoss(const float *render, const float *targetF, const uint8_t *target
                 float *grad, const LossScratch &ls, cudaStream_t s, const StepDesc *desc)
 {
     const SsimWindow &win = window();
-    static const bool sized = [] {
-        cudaFuncSetAttribute(lossKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(LossSmem)));
-        return true;
-    }();
-    (void)sized;
     dim3 g((width + kTW - 1) / kTW, (height + kTH - 1) / kTH);
-    { lossKernel<<<g, kThreads, sizeof(LossSmem), s>>>(render, targetF, targetU8, width, height, lambda, grad,
-                                                      ls.blockSums, desc, win); countLaunch(); }
+    { lossForwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, lambda, grad, ls.abc,
+                                             ls.blockSums, desc, win); countLaunch(); }
+    if (lambda > 0.0f)
+        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad, desc, win); countLaunch(); }
 }
 
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,

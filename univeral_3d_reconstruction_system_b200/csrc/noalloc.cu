@@ -1,19 +1,22 @@
 // noalloc.cu - the photometric loss on caller-owned device buffers, with no allocation in the call.
 //
 // No reference counterpart. u3dg_photometric_loss (photometricLoss, Loss.cpp:47-184) takes host
-// images and allocates its device buffers and scratch on every call. This variant runs the same loss
-// kernel and the same finalize kernel (loss.cu) on device pointers the caller owns; its temporaries
-// live in one file-scope device array, so the call makes no cudaMalloc, no cudaFree and no call into
-// an allocating library routine.
+// images and allocates its device buffers and SSIM scratch on every call. This variant runs the same
+// two loss kernels and the same finalize kernel (loss.cu) on device pointers the caller owns; its
+// temporaries live in one file-scope device array, so the call makes no cudaMalloc, no cudaFree and
+// no call into an allocating library routine.
 //
-// Scratch (gNoAllocScratch, 48 KB per device context that uses this entry point):
+// Scratch (gNoAllocScratch, 11.1 MB per device context that uses this entry point):
 //   [0, 3 * kMaxBlocks) doubles      per-block sums (L1, SSIM, squared error), 3 per loss block
 //   next 4 floats                    total, L1, SSIM, PSNR from the finalize kernel
+//   from a 256-byte boundary         the SSIM partial maps, 9 floats per pixel
 // Nothing in it has to start at zero: every element a call reads was written earlier in that call
-// (each loss block writes its three sums; the finalize kernel writes the four values).
+// (each loss block writes its three sums; with lambda > 0 the forward kernel writes all nine maps
+// of every pixel before the backward kernel reads them, and with lambda = 0 no kernel reads them;
+// the finalize kernel writes the four values).
 //
-// Limit: at most kMaxBlocks loss blocks of 32 x 16 pixels (for example 1280 x 800, or 1024 x 1024);
-// larger requests are rejected with U3DG_ERR_CAPACITY before anything is launched.
+// Limits: width * height <= kMaxPixels (640 x 480) and at most kMaxBlocks loss blocks (32 x 16
+// pixels each); larger requests are rejected with U3DG_ERR_CAPACITY before anything is launched.
 //
 // Set-up: the first call in each device context, with that device current, resolves the array's
 // address there with cudaGetSymbolAddress (which loads this module into the context) and keeps it
@@ -41,10 +44,12 @@ using namespace u3dg;
 
 namespace {
 
+constexpr size_t kMaxPixels = 640 * 480;
 constexpr int kMaxBlocks = 2048;
 constexpr size_t kSumsDoubles = 3 * size_t(kMaxBlocks);
-constexpr size_t kValsOffset = kSumsDoubles; // in doubles; 4 floats = 2 doubles
-constexpr size_t kScratchDoubles = kValsOffset + 2;
+constexpr size_t kValsOffset = kSumsDoubles;                           // in doubles; 4 floats = 2 doubles
+constexpr size_t kMapsOffset = (kValsOffset + 2 + 31) / 32 * 32;       // 256-byte boundary, in doubles
+constexpr size_t kScratchDoubles = kMapsOffset + (9 * kMaxPixels + 1) / 2;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double gNoAllocScratch[kScratchDoubles];
@@ -81,10 +86,9 @@ extern "C" int u3dg_photometric_loss_noalloc(const float *render, const float *t
     return guardedCall([&] {
         if (!render || !target || !grad || width <= 0 || height <= 0)
             throw StatusError(U3DG_ERR_INVALID_ARG, "invalid loss arguments");
-        const long long blocks64 = ((static_cast<long long>(width) + 31) / 32) * ((static_cast<long long>(height) + 15) / 16);
-        if (blocks64 > kMaxBlocks)
-            throw StatusError(U3DG_ERR_CAPACITY, "image needs more than 2048 loss blocks of 32x16 pixels (the "
-                                                 "no-allocation scratch holds the sums of 2048)");
+        const size_t pixels = size_t(width) * size_t(height);
+        if (pixels > kMaxPixels)
+            throw StatusError(U3DG_ERR_CAPACITY, "image larger than the 307200-pixel (640x480) no-allocation scratch");
         const int blocks = lossBlocks(width, height);
         if (blocks > kMaxBlocks)
             throw StatusError(U3DG_ERR_CAPACITY, "image needs more than 2048 loss blocks of 32x16 pixels");
@@ -108,7 +112,7 @@ extern "C" int u3dg_photometric_loss_noalloc(const float *render, const float *t
         }
         double *base = gScratchAddress[device];
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
-        const LossScratch ls{base, blocks};
+        const LossScratch ls{reinterpret_cast<float *>(base + kMapsOffset), base, blocks};
         float *vals = reinterpret_cast<float *>(base + kValsOffset);
         launchLoss(render, target, nullptr, width, height, lambda, grad, ls, s);
         launchLossFinalize(ls, width, height, lambda, nullptr, 0, nullptr, vals, vals + 3, s);
