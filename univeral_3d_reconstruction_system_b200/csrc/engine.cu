@@ -1190,12 +1190,12 @@ DensifyResult densifyOnDevice(TrainerImpl &t, std::mt19937 &rng)
     // A fresh distribution per call, as the reference constructs one per densifyAndPrune.
     std::normal_distribution<float> normal(0.0f, 1.0f);
     const size_t ns = size_t(splits) * 6;
-    t.hNormals.reserve(std::max<size_t>(ns, 1));
+    t.hNormals.resize(std::max<size_t>(ns, 1));
     for (size_t k = 0; k < ns; ++k)
-        t.hNormals.p[k] = normal(rng);
+        t.hNormals[k] = normal(rng);
     t.normals.reserve(std::max<size_t>(ns, 1));
     if (ns > 0)
-        U3DG_CUDA(cudaMemcpyAsync(t.normals.p, t.hNormals.p, ns * sizeof(float), cudaMemcpyHostToDevice, s));
+        U3DG_CUDA(cudaMemcpyAsync(t.normals.p, t.hNormals.data(), ns * sizeof(float), cudaMemcpyHostToDevice, s));
     const int other = 1 - t.cur;
     launchDensifyWrite(P, t.moment1(), t.moment2(), t.paramsOf(other, 0), t.paramsOf(other, 1), t.paramsOf(other, 2), n,
                        t.keep.p, t.keepScan.p, t.accCost.p, t.accScan.p, t.isSplit.p, t.splitScan.p, kept, t.normals.p,

@@ -321,7 +321,7 @@ struct TrainerImpl {
     DevBuf<int> keep, cost, costScan, accCost, accScan, isSplit, splitScan, keepScan, firstSecond, dScanPartial;
     DevBuf<float> normals;
     HostPinned<int> hCounts;
-    HostPinned<float> hNormals;
+    std::vector<float> hNormals; // split samples drawn on the host (pageable: copied once per densification)
 
     std::mt19937 rng;
     std::vector<int> order;

@@ -28,8 +28,15 @@ namespace u3dg {
 
 namespace {
 
+// Per-pixel state of the back-to-front replay. The colour behind the current entry enters the
+// gradient only through its dot product with dL/dpixel, so the state keeps that scalar (accd, the
+// running sum over channels of accum[ch] * dpix[ch]) and the last entry's colour dot product (lcd)
+// instead of three channels each: the recurrence accum = lastAlpha * lastColour + (1 - lastAlpha) *
+// accum is linear, so accd follows the same recurrence on the dot products. Three fewer multiply-adds
+// per channel per pair and eight fewer live registers for a thread's two pixels (no spills); the sums
+// differ from the per-channel form by rounding only (within the gradient tolerance).
 struct PixelState {
-    float T, acc0, acc1, acc2, lc0, lc1, lc2, lastAlpha;
+    float T, accd, lcd, lastAlpha;
     float fT, d0, d1, d2, bgDot, fy;
     int nC;
 };
@@ -50,20 +57,14 @@ __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const
     const float4 R = sR[jj];
     s.T = __fdiv_rn(s.T, __fsub_rn(1.0f, al));
     const float w = al * s.T;
-    float dAl = 0.0f;
-    s.acc0 = s.lastAlpha * s.lc0 + (1.0f - s.lastAlpha) * s.acc0;
-    s.lc0 = R.x;
-    dAl += (R.x - s.acc0) * s.d0;
+    // dAlpha = sum_ch (colour[ch] - accum[ch]) * dpix[ch] * T (Rasterizer.cpp:393-399), on dot products.
+    const float rd = R.x * s.d0 + R.y * s.d1 + R.z * s.d2;
+    s.accd = s.lastAlpha * s.lcd + (1.0f - s.lastAlpha) * s.accd;
+    s.lcd = rd;
+    float dAl = (rd - s.accd) * s.T;
     c[5] += w * s.d0;
-    s.acc1 = s.lastAlpha * s.lc1 + (1.0f - s.lastAlpha) * s.acc1;
-    s.lc1 = R.y;
-    dAl += (R.y - s.acc1) * s.d1;
     c[6] += w * s.d1;
-    s.acc2 = s.lastAlpha * s.lc2 + (1.0f - s.lastAlpha) * s.acc2;
-    s.lc2 = R.z;
-    dAl += (R.z - s.acc2) * s.d2;
     c[7] += w * s.d2;
-    dAl *= s.T;
     s.lastAlpha = al;
     // -finalT / (1 - alpha) * bgDot adds a signed zero when bgDot is 0 (black background), which leaves
     // dAl unchanged: skip the division then.
@@ -71,11 +72,12 @@ __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const
         dAl += -s.fT / (1.0f - al) * s.bgDot;
     if (raw > kMaxAlpha)
         return true; // clamped alpha: colour gradient only
-    c[8] += G * dAl;
+    const float t = G * dAl;
+    c[8] += t;
     // The mean and conic gradients are linear in the per-pixel moments of dPow: sum dPow dx, dPow dy,
     // dPow dx^2, dPow dx dy, dPow dy^2 here, and combine them with the conic once per list entry
     // (finishEntry) instead of once per pixel.
-    const float dPow = Q.w * dAl * G;
+    const float dPow = Q.w * t;
     const float pdx = dPow * dx, pdy = dPow * dy;
     c[0] += pdx;
     c[1] += pdy;
@@ -142,7 +144,7 @@ __device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix
     s.d2 = inside ? dLdRgb[pix * 3 + 2] : 0.0f;
     s.bgDot = bg[0] * s.d0 + bg[1] * s.d1 + bg[2] * s.d2;
     s.T = s.fT;
-    s.acc0 = s.acc1 = s.acc2 = s.lc0 = s.lc1 = s.lc2 = s.lastAlpha = 0.0f;
+    s.accd = s.lcd = s.lastAlpha = 0.0f;
     s.fy = fy;
 }
 
