@@ -10,14 +10,14 @@ backward. Checked per step, as one training step computes them:
   - image within 1e-5 absolute per channel, final transmittance within 1e-5, contributor counts exact
     (with culling, a count indexes the culled list: it must name the same last contributor);
   - per-parameter gradients of the L1 + 0.2 D-SSIM loss against the view's target within 1e-4
-    relative (floor: 1% of the group's largest magnitude) and the NDC densification statistic. At this
-    size a few near-cancelling sums of tens of thousands of pixels round past that bar in ANY other
-    summation order: the reference's own backward with all host threads (its default; CAS atomics in
-    arrival order) lands up to 1.58e-4 from its one-thread result on the scales of the 250k model, and
-    the quaternion gradients of the isotropic 300k model are rounding noise on both sides (zero in
-    exact arithmetic). So per group the bar is the larger of 1e-4 and twice the reference's own
-    multithreaded deviation from the oracle on the same step, for the worst element and for the
-    fraction of elements beyond 1e-4 (at least 1e-5 of them allowed).
+    relative (floor: 1% of the group's largest magnitude) for at least 99.99% of the elements, and
+    every element within 1e-3, and the same for the NDC densification statistic. At this size a few
+    near-cancelling sums of tens of thousands of pixels round past 1e-4 in ANY other summation order:
+    the reference's own backward with all host threads (its default; CAS atomics in arrival order)
+    lands up to 1.6e-4 from its one-thread result (the oracle) on the scales and quaternions of the
+    250k model, a different amount on every run; the test prints that spread beside the GPU's. The
+    quaternion gradients of the isotropic 300k model are zero in exact arithmetic and rounding noise
+    on every side: they are checked to be negligible instead.
 Models: the bench workload (initGaussiansFromPoints of every true centre plus 50k re-samples:
 isotropic, opacity 0.1) and the ground truth itself (anisotropic, opacity 0.3-1)."""
 from __future__ import annotations
@@ -141,14 +141,19 @@ def test_high_step_matches_oracle(u3dg, oracle, reference, high, model):
     g = r.backward(model, dl, None, ndc)
     og, ondc = o.backward(dl)
     spread = _reference_spread(reference, model, cam, st, dl, og, ondc)
+    isotropic = bool(np.all(model.scales == model.scales[:, :1]) and np.all(model.quats[:, 1:] == 0))
     for name in GROUPS + ("ndc",):
         got = _ratios(ndc, ondc) if name == "ndc" else _ratios(getattr(g, name), getattr(og, name))
         worst, frac = float(got.max()), float(np.mean(got > 1.0))
         ref_worst, ref_frac = spread[name]
         print(f"{name}: worst {worst:.3g} (reference threads {ref_worst:.3g}), beyond 1e-4: {frac:.2e} "
               f"(reference threads {ref_frac:.2e})")
-        assert worst <= max(1.0, 2.0 * ref_worst), (name, worst, ref_worst)
-        assert frac <= max(1e-5, 2.0 * ref_frac), (name, frac, ref_frac)
+        if name == "quats" and isotropic:
+            scale = max(float(np.max(np.abs(og.means))), float(np.max(np.abs(og.scales))))
+            assert float(np.max(np.abs(g.quats))) <= 1e-3 * scale
+            assert float(np.max(np.abs(og.quats))) <= 1e-3 * scale
+            continue
+        assert frac <= 1e-4 and worst <= 10.0, (name, worst, frac)
 
     # Culling off at the unit boundary: the reference's own lists and contributor counts.
     r.set_tile_culling(False)

@@ -89,6 +89,7 @@ template <int DB>
 __global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int shift, int *hist,
                                                             int G)
 {
+    pdlEntry();
     constexpr int R = 1 << DB;
     __shared__ int counts[R];
     for (int d = threadIdx.x; d < R; d += kThreads)
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys
 // One block per digit: exclusive scan of that digit's row of G block counts; rowTotals[d] = sum.
 __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G, int *rowTotals)
 {
+    pdlEntry();
     int *row = hist + size_t(blockIdx.x) * G;
     int carry = 0;
     for (int c0 = 0; c0 < G; c0 += kThreads) {
@@ -135,6 +137,7 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
                                                                int shift, const int *hist, const int *rowTotals, int G,
                                                                TileFinish fin)
 {
+    pdlEntry();
     constexpr int R = 1 << DB;
     __shared__ uint8_t warpCounts[kWarps][R];
     __shared__ int base[R];
@@ -226,6 +229,7 @@ constexpr int kScanTile = kThreads * 8;
 
 __global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int n, int *partial)
 {
+    pdlEntry();
     const int base = blockIdx.x * kScanTile;
     int s = 0;
 #pragma unroll
@@ -242,6 +246,7 @@ __global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int 
 
 __global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int B)
 {
+    pdlEntry();
     int carry = 0;
     for (int c0 = 0; c0 < B; c0 += kThreads) {
         const int i = c0 + threadIdx.x;
@@ -258,6 +263,7 @@ __global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int 
 
 __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B)
 {
+    pdlEntry();
     const int base = blockIdx.x * kScanTile + threadIdx.x * 8;
     int v[8];
     int s = 0;
@@ -354,6 +360,7 @@ __device__ __forceinline__ void cullSpan(const CullShape &c, const int4 &q, int 
 __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
                                  int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab)
 {
+    pdlEntry();
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n)
         return;
@@ -383,6 +390,7 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
 // clears it). iteration identifies the aborted step for the host.
 __global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int iteration, const StepDesc *desc)
 {
+    pdlEntry();
     if (desc)
         iteration = desc->iteration;
     const int t = *total;
@@ -405,6 +413,7 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
                                                   const BinCounts *c, int tilesX, const SplatRec *cullRec, int tileSize,
                                                   const uint32_t *rowTab, uint32_t *keys, int *emitGid)
 {
+    pdlEntry();
     const int total = c->effTotal;
     if (total <= 0)
         return;
@@ -491,6 +500,7 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
 
 __global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c, int *list)
 {
+    pdlEntry();
     const int total = c->effTotal;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x)
         list[s] = emitGid[sortedEmit[s]];
@@ -498,6 +508,7 @@ __global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, c
 
 __global__ void tileOffsetsKernel(const uint32_t *sortedKeys, const BinCounts *c, int tiles, int *tileOffsets)
 {
+    pdlEntry();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > tiles)
         return;
@@ -539,16 +550,16 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     int passes = 0;
     for (int shift = 0; shift < bits; shift += db, ++passes) {
         if (wide) {
-            { radixHistKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
-            { radixRowScanKernel<<<1 << kWideBits, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
+            { launchPdl(radixHistKernel<kWideBits>, G, kThreads, 0, s, kin, nDev, shift, hist, G); countLaunch(); }
+            { launchPdl(radixRowScanKernel, 1 << kWideBits, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
             if (fin != nullptr)
-                { radixScatterKernel<kWideBits, true><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, *fin); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits, true>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, *fin); countLaunch(); }
             else
-                { radixScatterKernel<kWideBits><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         } else {
-            { radixHistKernel<8><<<G, kThreads, 0, s>>>(kin, nDev, shift, hist, G); countLaunch(); }
-            { radixRowScanKernel<<<1 << 8, kThreads, 0, s>>>(hist, G, rowTotals); countLaunch(); }
-            { radixScatterKernel<8><<<G, kThreads, 0, s>>>(kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+            { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, kin, nDev, shift, hist, G); countLaunch(); }
+            { launchPdl(radixRowScanKernel, 1 << 8, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
+            { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         }
         uint32_t *nk = kin;
         kin = kout;
@@ -570,9 +581,9 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
         cudaMemsetAsync(out, 0, sizeof(int), s);
         return;
     }
-    { scanReduceKernel<<<B, kThreads, 0, s>>>(in, n, partial); countLaunch(); }
-    { scanPartialKernel<<<1, kThreads, 0, s>>>(partial, B); countLaunch(); }
-    { scanDownsweepKernel<<<B, kThreads, 0, s>>>(in, out, n, partial, B); countLaunch(); }
+    { launchPdl(scanReduceKernel, B, kThreads, 0, s, in, n, partial); countLaunch(); }
+    { launchPdl(scanPartialKernel, 1, kThreads, 0, s, partial, B); countLaunch(); }
+    { launchPdl(scanDownsweepKernel, B, kThreads, 0, s, in, out, n, partial, B); countLaunch(); }
 }
 
 size_t cullRowEntries(size_t n) { return n * kCullRows; }
@@ -581,22 +592,23 @@ void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *ra
                       int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s)
 {
     if (n > 0)
-        { rankCountsKernel<<<grid(n, 256), 256, 0, s>>>(sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf, rowTab); countLaunch(); }
+        { launchPdl(rankCountsKernel, grid(n, 256), 256, 0, s, sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf, rowTab); countLaunch(); }
 }
 
 namespace {
-__global__ void setCountKernel(BinCounts *c, int n) { c->n = n; }
+__global__ void setCountKernel(BinCounts *c, int n) {
+    pdlEntry(); c->n = n; }
 } // namespace
 
 void launchSetCount(BinCounts *c, int n, cudaStream_t s)
 {
-    { setCountKernel<<<1, 1, 0, s>>>(c, n); countLaunch(); }
+    { launchPdl(setCountKernel, 1, 1, 0, s, c, n); countLaunch(); }
 }
 
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
                          const StepDesc *desc)
 {
-    { capacityKernel<<<1, 1, 0, s>>>(total, capacity, c, iteration, desc); countLaunch(); }
+    { launchPdl(capacityKernel, 1, 1, 0, s, total, capacity, c, iteration, desc); countLaunch(); }
 }
 
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
@@ -604,15 +616,15 @@ void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, in
                 cudaStream_t s)
 {
     if (n > 0 && capacity > 0)
-        { emitKernel<<<std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(sortedIds, offs, rect, n, c, tilesX, cullRec, tileSize, rowTab, keys, emitGid); countLaunch(); }
+        { launchPdl(emitKernel, std::min(grid((long long)(n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s, sortedIds, offs, rect, n, c, tilesX, cullRec, tileSize, rowTab, keys, emitGid); countLaunch(); }
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
                         int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s)
 {
     if (capacity > 0)
-        { finalizeKernel<<<std::min(grid(capacity, 256), 148 * 16), 256, 0, s>>>(sortedEmit, emitGid, c, list); countLaunch(); }
-    { tileOffsetsKernel<<<grid(tiles + 1, 256), 256, 0, s>>>(sortedKeys, c, tiles, tileOffsets); countLaunch(); }
+        { launchPdl(finalizeKernel, std::min(grid(capacity, 256), 148 * 16), 256, 0, s, sortedEmit, emitGid, c, list); countLaunch(); }
+    { launchPdl(tileOffsetsKernel, grid(tiles + 1, 256), 256, 0, s, sortedKeys, c, tiles, tileOffsets); countLaunch(); }
 }
 
 } // namespace u3dg

@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
                                                      int tilesX, int tilesY, const float *shRestCoef, int shDegree,
                                                      float3 camPos, ProjOut out, const StepDesc *desc)
 {
+    pdlEntry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -183,6 +184,7 @@ __global__ void __launch_bounds__(256) partialSumKernel(const float *partial, in
                                                         const int *offs, const uint32_t *sortedIds, int n,
                                                         const BinCounts *counts, float *g2d)
 {
+    pdlEntry();
     if (counts != nullptr && counts->abortIter >= 0)
         return;
     const int lane = threadIdx.x & 31;
@@ -262,6 +264,7 @@ __global__ void __launch_bounds__(256) partialSumKernel(const float *partial, in
 template <bool kAdam>
 __global__ void __launch_bounds__(256, U3DG_CHAIN_MIN_BLOCKS) chainKernel(ChainArgs a)
 {
+    pdlEntry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n || (a.counts != nullptr && a.counts->abortIter >= 0))
         return;
@@ -590,19 +593,19 @@ void launchProject(const Params &P, int n, const u3dg_camera &cam, const u3dg_ra
     }
     if (desc)
         shDegree = 0;
-    { projectKernel<<<blocks(n, 256), 256, 0, s>>>(P, n, cam, st, tilesX, tilesY, shRest, shDegree, camPos, out, desc); countLaunch(); }
+    { launchPdl(projectKernel, blocks(n, 256), 256, 0, s, P, n, cam, st, tilesX, tilesY, shRest, shDegree, camPos, out, desc); countLaunch(); }
 }
 
 void launchChain(const ChainArgs &a, bool adam, cudaStream_t s)
 {
     if (a.n <= 0)
         return;
-    { partialSumKernel<<<std::min(blocks((long long)(a.n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s>>>(
+    { launchPdl(partialSumKernel, std::min(blocks((long long)(a.n + 31) / 32 * 32, 256), 148 * 16), 256, 0, s, 
           a.partial, std::max(a.subSlots, 1), a.subStride, a.offs, a.sortedIds, a.n, a.counts, a.g2d); countLaunch(); }
     if (adam)
-        { chainKernel<true><<<blocks(a.n, 256), 256, 0, s>>>(a); countLaunch(); }
+        { launchPdl(chainKernel<true>, blocks(a.n, 256), 256, 0, s, a); countLaunch(); }
     else
-        { chainKernel<false><<<blocks(a.n, 256), 256, 0, s>>>(a); countLaunch(); }
+        { launchPdl(chainKernel<false>, blocks(a.n, 256), 256, 0, s, a); countLaunch(); }
 }
 
 void launchAdamSegment(float *p, const float *g, float *m, float *v, int len, float stepSize, float invSqrtBc2,

@@ -3,7 +3,40 @@
 
 #include "common.cuh"
 
+#include <utility>
+
 namespace u3dg {
+
+// Programmatic dependent launch (sm_90+): the kernels of a training step are launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so the GPU may schedule a kernel's CTAs while
+// the previous kernel in the stream drains; each such kernel starts with pdlEntry(), which waits until
+// the previous kernel has completed and its memory is visible (griddepcontrol.wait) and then lets the
+// next kernel be scheduled (griddepcontrol.launch_dependents). Ordering is the plain stream order's;
+// what overlaps is one kernel's launch and CTA set-up with the previous one's tail. In a kernel
+// launched without the attribute both instructions do nothing.
+__device__ __forceinline__ void pdlEntry()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+
+// Launches `kernel` on stream s with programmatic stream serialisation (see pdlEntry; the kernel must
+// call pdlEntry() before it reads anything an earlier kernel wrote).
+template <typename... KArgs, typename... Args>
+inline void launchPdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Device-side sizes of one bin pass. The host never waits for them inside a step: it reads the
 // struct back asynchronously and checks it one step later.

@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kThreads) lossForwardKernel(const float *rende
                                                               float *grad, float *abc, double *blockSums,
                                                               const StepDesc *desc, const SsimWindow cWin)
 {
+    pdlEntry();
     if (desc)
         targetU8 = desc->target;
     __shared__ float sx[kIH][kIW], sy[kIH][kIW];
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
                                                                float *grad, const StepDesc *desc,
                                                                const SsimWindow cWin)
 {
+    pdlEntry();
     if (desc)
         targetU8 = desc->target;
     __shared__ float sm[3][kIH][kIW];
@@ -235,6 +237,7 @@ __global__ void __launch_bounds__(kThreads) lossFinalizeKernel(const double *blo
                                                                const BinCounts *counts, float *out3, float *psnrOut,
                                                                const StepDesc *desc)
 {
+    pdlEntry();
     if (desc)
         iteration = desc->iteration + 1;
     if (counts != nullptr && counts->abortIter >= 0)
@@ -336,16 +339,16 @@ void launchLoss(const float *render, const float *targetF, const uint8_t *target
 {
     const SsimWindow &win = window();
     dim3 g((width + kTW - 1) / kTW, (height + kTH - 1) / kTH);
-    { lossForwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, lambda, grad, ls.abc,
+    { launchPdl(lossForwardKernel, g, kThreads, 0, s, render, targetF, targetU8, width, height, lambda, grad, ls.abc,
                                              ls.blockSums, desc, win); countLaunch(); }
     if (lambda > 0.0f)
-        { lossBackwardKernel<<<g, kThreads, 0, s>>>(render, targetF, targetU8, width, height, ls.abc, grad, desc, win); countLaunch(); }
+        { launchPdl(lossBackwardKernel, g, kThreads, 0, s, render, targetF, targetU8, width, height, ls.abc, grad, desc, win); countLaunch(); }
 }
 
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
                         const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s, const StepDesc *desc)
 {
-    { lossFinalizeKernel<<<1, kThreads, 0, s>>>(ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
+    { launchPdl(lossFinalizeKernel, 1, kThreads, 0, s, ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
                                               counts, out3, psnrOut, desc); countLaunch(); }
 }
 

@@ -120,6 +120,7 @@ template <int PB, int BD>
 __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_FWD_MIN_BLOCKS) compositeForwardKernel(RasterArgs a, float *rgb, float *finalT,
                                                                               int *nContrib)
 {
+    pdlEntry();
     using S = RasterShape<PB, BD>;
     constexpr int NB = S::NB, NW = S::NW, NG = S::NG;
     __shared__ float4 sP[NB]; // mx, my, powMin, ey
@@ -154,6 +155,7 @@ __device__ __forceinline__ int lengthBucket(unsigned len)
 __global__ void __launch_bounds__(1024) blockOrderKernel(const int *tileOffsets, int blocksX, int blocksY, int pb,
                                                          int tileSize, int tilesX, int *order)
 {
+    pdlEntry();
     __shared__ int count[kOrderBuckets];
     __shared__ int cursor[kOrderBuckets];
     const int units = blocksX * blocksY;
@@ -201,7 +203,7 @@ void launchBlockOrder(const RasterArgs &a, int *order, cudaStream_t s)
     if (units <= 0)
         return;
     const int pb = a.tileSize <= 8 ? 8 : 16;
-    { blockOrderKernel<<<1, 1024, 0, s>>>(a.tileOffsets, a.blocksX, a.blocksY, pb, a.tileSize, a.tilesX, order); countLaunch(); }
+    { launchPdl(blockOrderKernel, 1, 1024, 0, s, a.tileOffsets, a.blocksX, a.blocksY, pb, a.tileSize, a.tilesX, order); countLaunch(); }
 }
 
 template <int PB, int BD>
@@ -214,7 +216,7 @@ static void launchForward(const RasterArgs &a, float *rgb, float *finalT, int *n
     RasterArgs f = a;
     if (units <= ctas)
         f.counters = nullptr;
-    { compositeForwardKernel<PB, BD><<<std::min(units, ctas), RasterShape<PB>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
+    { launchPdl(compositeForwardKernel<PB, BD>, std::min(units, ctas), RasterShape<PB>::NT, 0, s, f, rgb, finalT, nContrib); countLaunch(); }
 }
 
 // 8x8 CTAs over the lists of larger tiles: one CTA per pixel block in natural order, as many waves as
@@ -226,7 +228,7 @@ static void launchForwardSplit(const RasterArgs &a, float *rgb, float *finalT, i
     f.blocksX = (a.width + 7) / 8;
     f.blocksY = (a.height + 7) / 8;
     f.counters = nullptr;
-    { compositeForwardKernel<8, BD><<<f.blocksX * f.blocksY, RasterShape<8>::NT, 0, s>>>(f, rgb, finalT, nContrib); countLaunch(); }
+    { launchPdl(compositeForwardKernel<8, BD>, f.blocksX * f.blocksY, RasterShape<8>::NT, 0, s, f, rgb, finalT, nContrib); countLaunch(); }
 }
 
 void launchCompositeForward(const RasterArgs &a, float *rgb, float *finalT, int *nContrib, cudaStream_t s)

@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) comp
                                                                               const float *finalTIn,
                                                                               const int *nContribIn, float *partial)
 {
+    pdlEntry();
     using S = RasterShape<PB, BD>;
     constexpr int NB = S::NB, NW = S::NW, NG = S::NG;
     __shared__ float4 sP[NB];
@@ -321,7 +322,7 @@ static void launchBackward(const RasterArgs &a, const float *dLdRgb, const float
         return residentCtas(compositeBackwardKernel<PB, BD>, S::NT, smem);
     }();
     const int units = a.blocksX * a.blocksY;
-    { compositeBackwardKernel<PB, BD><<<std::min(units, ctas), S::NT, smem, s>>>(a, dLdRgb, finalT, nContrib, partial); countLaunch(); }
+    { launchPdl(compositeBackwardKernel<PB, BD>, std::min(units, ctas), S::NT, smem, s, a, dLdRgb, finalT, nContrib, partial); countLaunch(); }
 }
 
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
