@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 
 namespace u3dg {
 
@@ -42,6 +43,8 @@ struct PixelState {
 };
 
 // One back-to-front step of Rasterizer.cpp:385-416 for one pixel; adds its 9 contributions to c.
+// kBg: the background is not black (its term enters dAlpha).
+template <bool kBg>
 __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const float4 *sR, int jj, float dx,
                                          const ColumnTerms &ct, float minA, PixelState &s, float c[kG2d])
 {
@@ -59,30 +62,30 @@ __device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const
     const float w = al * s.T;
     // dAlpha = sum_ch (colour[ch] - accum[ch]) * dpix[ch] * T (Rasterizer.cpp:393-399), on dot products.
     const float rd = R.x * s.d0 + R.y * s.d1 + R.z * s.d2;
-    s.accd = s.lastAlpha * s.lcd + (1.0f - s.lastAlpha) * s.accd;
+    s.accd = s.accd + s.lastAlpha * (s.lcd - s.accd); // lastAlpha * lcd + (1 - lastAlpha) * accd
     s.lcd = rd;
     float dAl = (rd - s.accd) * s.T;
     c[5] += w * s.d0;
     c[6] += w * s.d1;
     c[7] += w * s.d2;
     s.lastAlpha = al;
-    // -finalT / (1 - alpha) * bgDot adds a signed zero when bgDot is 0 (black background), which leaves
-    // dAl unchanged: skip the division then.
-    if (s.bgDot != 0.0f)
+    // -finalT / (1 - alpha) * bgDot: with a black background (kBg false) it would add a signed zero,
+    // which leaves dAl unchanged, so those launches compile it out.
+    if (kBg)
         dAl += -s.fT / (1.0f - al) * s.bgDot;
     if (raw > kMaxAlpha)
         return true; // clamped alpha: colour gradient only
     const float t = G * dAl;
     c[8] += t;
     // The mean and conic gradients are linear in the per-pixel moments of dPow: sum dPow dx, dPow dy,
-    // dPow dx^2, dPow dx dy, dPow dy^2 here, and combine them with the conic once per list entry
-    // (finishEntry) instead of once per pixel.
+    // dPow dx^2, dPow dx dy, dPow dy^2, and combine them with the conic once per list entry
+    // (finishEntry) instead of once per pixel. A thread's two pixels share dx, so the pixels add
+    // sum dPow (c[0]), dPow dy (c[1]) and dPow dy^2 (c[4]) only; the thread multiplies by dx once
+    // (c[0] -> dx sum dPow, c[2] = dx^2 sum dPow, c[3] = dx sum dPow dy) before the warp sum.
     const float dPow = Q.w * t;
-    const float pdx = dPow * dx, pdy = dPow * dy;
-    c[0] += pdx;
+    const float pdy = dPow * dy;
+    c[0] += dPow;
     c[1] += pdy;
-    c[2] += pdx * dx;
-    c[3] += pdx * dy;
     c[4] += pdy * dy;
     return true;
 }
@@ -148,7 +151,7 @@ __device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix
     s.fy = fy;
 }
 
-template <int PB, int BD>
+template <int PB, int BD, bool kBg>
 __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int by, const float *dLdRgb,
                                               const float *finalTIn, const int *nContribIn, float *partial,
                                               float4 *sP, float4 *sQ, float4 *sR,
@@ -228,9 +231,12 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                     const float dx = __fsub_rn(P.x, fx);
                     const ColumnTerms ct = columnTerms(Q, dx);
                     if (j < s0.nC)
-                        act |= pairGrad(P, Q, sR, jj, dx, ct, minA, s0, c);
+                        act |= pairGrad<kBg>(P, Q, sR, jj, dx, ct, minA, s0, c);
                     if (j < s1.nC)
-                        act |= pairGrad(P, Q, sR, jj, dx, ct, minA, s1, c);
+                        act |= pairGrad<kBg>(P, Q, sR, jj, dx, ct, minA, s1, c);
+                    c[3] = dx * c[1];
+                    c[0] = dx * c[0];
+                    c[2] = dx * c[0]; // c[0] already holds dx sum dPow
                 }
                 if (__any_sync(0xffffffffu, act)) {
                     float v8;
@@ -276,7 +282,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
 #define U3DG_BWD_CARVEOUT -1
 #endif
 
-template <int PB, int BD>
+template <int PB, int BD, bool kBg>
 __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) compositeBackwardKernel(RasterArgs a, const float *dLdRgb,
                                                                               const float *finalTIn,
                                                                               const int *nContribIn, float *partial)
@@ -293,7 +299,7 @@ __global__ void __launch_bounds__(RasterShape<PB>::NT, U3DG_BWD_MIN_BLOCKS) comp
     const int units = a.blocksX * a.blocksY;
     int *counter = a.counters + 2; // backward: counters[2..3]
     for (int b = nextBlock(a, counter, &sNext); b < units; b = nextBlock(a, counter, &sNext))
-        backwardBlock<PB, BD>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, sP, sQ, sR,
+        backwardBlock<PB, BD, kBg>(a, b % a.blocksX, b / a.blocksX, dLdRgb, finalTIn, nContribIn, partial, sP, sQ, sR,
                               mask, sMax, sWarp);
 }
 
@@ -311,18 +317,18 @@ int residentCtas(K kernel, int threads, size_t smem)
 
 } // namespace
 
-template <int PB, int BD>
+template <int PB, int BD, bool kBg>
 static void launchBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
                            float *partial, cudaStream_t s)
 {
     using S = RasterShape<PB, BD>;
     const size_t smem = size_t(S::NW) * S::NB * kG2d * sizeof(float); // 18 KB (BD 1) or 36 KB (BD 2) at PB 16
     static const int ctas = [&] {
-        cudaFuncSetAttribute(compositeBackwardKernel<PB, BD>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        return residentCtas(compositeBackwardKernel<PB, BD>, S::NT, smem);
+        cudaFuncSetAttribute(compositeBackwardKernel<PB, BD, kBg>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        return residentCtas(compositeBackwardKernel<PB, BD, kBg>, S::NT, smem);
     }();
     const int units = a.blocksX * a.blocksY;
-    { launchPdl(compositeBackwardKernel<PB, BD>, std::min(units, ctas), S::NT, smem, s, a, dLdRgb, finalT, nContrib, partial); countLaunch(); }
+    { launchPdl(compositeBackwardKernel<PB, BD, kBg>, std::min(units, ctas), S::NT, smem, s, a, dLdRgb, finalT, nContrib, partial); countLaunch(); }
 }
 
 void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const float *finalT, const int *nContrib,
@@ -331,12 +337,20 @@ void launchCompositeBackward(const RasterArgs &a, const float *dLdRgb, const flo
     if (a.blocksX * a.blocksY <= 0)
         return;
     const bool deep = a.backwardDepth >= 2;
-    if (a.tileSize <= 8)
-        deep ? launchBackward<8, 2>(a, dLdRgb, finalT, nContrib, partial, s)
-             : launchBackward<8, 1>(a, dLdRgb, finalT, nContrib, partial, s);
+    const bool bg = a.bg[0] != 0.0f || a.bg[1] != 0.0f || a.bg[2] != 0.0f;
+    auto run = [&](auto kBg) {
+        constexpr bool B = decltype(kBg)::value;
+        if (a.tileSize <= 8)
+            deep ? launchBackward<8, 2, B>(a, dLdRgb, finalT, nContrib, partial, s)
+                 : launchBackward<8, 1, B>(a, dLdRgb, finalT, nContrib, partial, s);
+        else
+            deep ? launchBackward<16, 2, B>(a, dLdRgb, finalT, nContrib, partial, s)
+                 : launchBackward<16, 1, B>(a, dLdRgb, finalT, nContrib, partial, s);
+    };
+    if (bg)
+        run(std::true_type{});
     else
-        deep ? launchBackward<16, 2>(a, dLdRgb, finalT, nContrib, partial, s)
-             : launchBackward<16, 1>(a, dLdRgb, finalT, nContrib, partial, s);
+        run(std::false_type{});
 }
 
 } // namespace u3dg
