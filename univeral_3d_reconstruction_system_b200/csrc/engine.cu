@@ -41,6 +41,30 @@ unsigned long long allocEpoch() { return gAllocEpoch.load(std::memory_order_rela
 
 void bumpAllocEpoch() { gAllocEpoch.fetch_add(1, std::memory_order_relaxed); }
 
+void DeviceSlab::commit()
+{
+    if (items.empty())
+        return;
+    auto slice = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t sum = 0;
+    for (const Item &it : items)
+        sum += slice(it.bytes);
+    void *base = nullptr;
+    const cudaError_t e = cudaMalloc(&base, sum);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw StatusError(U3DG_ERR_OOM, "cudaMalloc of " + std::to_string(sum) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    bases.push_back(base);
+    total += sum;
+    size_t off = 0;
+    for (const Item &it : items) {
+        it.adopt(it.buf, static_cast<char *>(base) + off, it.count);
+        off += slice(it.bytes);
+    }
+    items.clear();
+}
+
 static thread_local std::string tLastError;
 
 int setError(int code, const std::string &msg)
@@ -94,21 +118,40 @@ void RasterWorkspace::clearCounts(cudaStream_t stream)
     U3DG_CUDA(cudaMemcpyAsync(counts.p, zero.p, sizeof(BinCounts), cudaMemcpyHostToDevice, stream));
 }
 
-void RasterWorkspace::reserveIntersections(size_t capacity)
+size_t RasterWorkspace::checkedIntersections(size_t capacity)
 {
     capacity = std::max<size_t>(capacity, 1024);
     if (capacity > size_t(INT_MAX / 16))
         throw StatusError(U3DG_ERR_CAPACITY, "tile-Gaussian intersections exceed the supported 1.3e8");
+    return capacity;
+}
+
+template <class F>
+void RasterWorkspace::eachIntersectionBuffer(size_t capacity, F &&f)
+{
+    f(iKeys0, capacity);
+    f(iKeys1, capacity);
+    f(iVals0, capacity);
+    f(iVals1, capacity);
+    f(emitGid, capacity);
+    f(list, capacity);
+    f(partial, capacity * kG2d * size_t(partialSlots));
+}
+
+void RasterWorkspace::reserveIntersections(size_t capacity)
+{
+    capacity = checkedIntersections(capacity);
     if (int(capacity) <= icap && iKeys0.p)
         return;
-    iKeys0.reserve(capacity, true);
-    iKeys1.reserve(capacity, true);
-    iVals0.reserve(capacity, true);
-    iVals1.reserve(capacity, true);
-    emitGid.reserve(capacity, true);
-    list.reserve(capacity, true);
-    partial.reserve(capacity * kG2d * size_t(partialSlots), true);
+    eachIntersectionBuffer(capacity, [](auto &b, size_t c) { b.reserve(c, true); });
     icap = int(capacity);
+}
+
+void RasterWorkspace::planIntersections(DeviceSlab &slab, size_t capacity)
+{
+    capacity = checkedIntersections(capacity);
+    eachIntersectionBuffer(capacity, [&](auto &b, size_t c) { slab.add(b, c); });
+    icap = std::max(icap, int(capacity));
 }
 
 void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
@@ -134,26 +177,49 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
     launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
 }
 
+template <class F>
+void RasterWorkspace::eachGaussianBuffer(size_t nn, F &&f)
+{
+    f(rec, nn);
+    f(depthKey, nn);
+    f(sortKeys, nn);
+    f(sortVals0, nn);
+    f(sortVals1, nn);
+    f(depth, nn);
+    f(rect, nn);
+    f(radius, nn);
+    f(rankOf, nn);
+    f(rowTab, cullRowEntries(nn));
+    f(cnt, nn);
+    f(offs, nn + 1);
+    f(scanPartial, scanPartialEntries(int(nn)) + 1);
+    f(flags, nn);
+    f(cov2d, nn);
+    f(g2d, nn * kG2d);
+    f(hist, std::max(radixHistEntries(std::max(int(nn), icap)), size_t(256)));
+}
+
 void RasterWorkspace::reserveGaussians(size_t nn)
 {
-    nn = std::max<size_t>(nn, 1);
-    rec.reserve(nn);
-    depthKey.reserve(nn);
-    sortKeys.reserve(nn);
-    sortVals0.reserve(nn);
-    sortVals1.reserve(nn);
-    depth.reserve(nn);
-    rect.reserve(nn);
-    radius.reserve(nn);
-    rankOf.reserve(nn);
-    rowTab.reserve(cullRowEntries(nn));
-    cnt.reserve(nn);
-    offs.reserve(nn + 1);
-    scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
-    flags.reserve(nn);
-    cov2d.reserve(nn);
-    g2d.reserve(nn * kG2d);
-    hist.reserve(std::max(radixHistEntries(std::max(int(nn), icap)), size_t(256)));
+    eachGaussianBuffer(std::max<size_t>(nn, 1), [](auto &b, size_t c) { b.reserve(c); });
+}
+
+void RasterWorkspace::planGaussians(DeviceSlab &slab, size_t nn)
+{
+    eachGaussianBuffer(std::max<size_t>(nn, 1), [&](auto &b, size_t c) { slab.add(b, c); });
+}
+
+void RasterWorkspace::planPixels(DeviceSlab &slab, size_t pixels, int tx, int ty, int tileSize)
+{
+    // The sizes bin() and composite() reserve for such a view.
+    slab.add(rgb, pixels * 3);
+    slab.add(finalT, pixels);
+    slab.add(nContrib, pixels);
+    slab.add(tileOffsets, size_t(tx) * ty + 1);
+    slab.add(rowTotals, size_t(radixDigits()));
+    const int pb = tileSize <= 8 ? 8 : 16;
+    const int per = tileSize > pb ? tileSize / pb : 1;
+    slab.add(blockOrder, size_t(std::max(1, tx * per * ty * per)));
 }
 
 void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *desc)
@@ -321,26 +387,53 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
     n = int(initial.count);
     cap = std::max<size_t>(size_t(std::max(o.max_gaussians, 0)), initial.count);
     cap = std::max<size_t>(cap, 1);
-    for (auto &a : arena)
-        a.reserve(42 * cap, true);
-    U3DG_CUDA(cudaMemsetAsync(arena[cur].p, 0, 42 * cap * sizeof(float), stream));
-    copyModelToArena(arena[cur].p, cap, initial, stream);
-    gradAccum.reserve(cap, true);
-    gradCount.reserve(cap, true);
-    U3DG_CUDA(cudaMemsetAsync(gradAccum.p, 0, cap * sizeof(float), stream));
-    U3DG_CUDA(cudaMemsetAsync(gradCount.p, 0, cap * sizeof(int), stream));
     size_t total = 0, maxP = 1;
+    int maxTx = 1, maxTy = 1, maxLossBlocks = 1;
+    const int ts = o.raster.tile_size;
     for (int k = 0; k < count; ++k) {
         checkCamera(imgs[k].camera);
         if (!imgs[k].rgb)
             throw StatusError(U3DG_ERR_INVALID_ARG, "image " + std::to_string(k) + " has no pixels");
-        cams.push_back(imgs[k].camera);
+        const u3dg_camera &c = imgs[k].camera;
+        cams.push_back(c);
         imageOffset.push_back(total);
-        const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
+        const size_t P = size_t(c.width) * c.height;
         total += P * 3;
         maxP = std::max(maxP, P);
+        maxTx = std::max(maxTx, (c.width + ts - 1) / ts);
+        maxTy = std::max(maxTy, (c.height + ts - 1) / ts);
+        maxLossBlocks = std::max(maxLossBlocks, lossBlocks(c.width, c.height));
     }
-    images.reserve(std::max<size_t>(total, 1), true);
+    // Everything a step, an evaluation or a densification needs, sized for the capacity and the
+    // largest view, in one device allocation: nothing is allocated during a schedule (allocations wait
+    // for the device), and creation pays for one cudaMalloc instead of one per buffer. Intersection
+    // buffers start at 16 tiles per Gaussian at the capacity and grow on demand.
+    for (auto &a : arena)
+        slab.add(a, 42 * cap);
+    slab.add(gradAccum, cap);
+    slab.add(gradCount, cap);
+    slab.add(images, std::max<size_t>(total, 1));
+    slab.add(dLoss, maxP * 3);
+    slab.add(abc, maxP * 9);
+    slab.add(lossBlockSums, size_t(maxLossBlocks) * 3);
+    slab.add(dStats, 1);
+    slab.add(descDev, kGraphSteps);
+    slab.add(statusDev, kGraphSteps);
+    const int per = ts > 16 ? ts / 16 : 1;
+    ws.partialSlots = std::max(ws.partialSlots, per * per);
+    ws.planIntersections(slab, std::max<size_t>(size_t(1) << 20, 16 * cap));
+    ws.planGaussians(slab, cap);
+    ws.planPixels(slab, maxP, maxTx, maxTy, ts);
+    for (DevBuf<int> *b : {&keep, &cost, &costScan, &accCost, &accScan, &isSplit, &splitScan, &keepScan})
+        slab.add(*b, cap + 1);
+    slab.add(firstSecond, 2);
+    slab.add(dScanPartial, scanPartialEntries(int(cap)) + 1);
+    slab.add(normals, 6 * cap);
+    slab.commit();
+    U3DG_CUDA(cudaMemsetAsync(arena[cur].p, 0, 42 * cap * sizeof(float), stream));
+    copyModelToArena(arena[cur].p, cap, initial, stream);
+    U3DG_CUDA(cudaMemsetAsync(gradAccum.p, 0, cap * sizeof(float), stream));
+    U3DG_CUDA(cudaMemsetAsync(gradCount.p, 0, cap * sizeof(int), stream));
     if (!backgroundUpload || count == 0) {
         for (int k = 0; k < count; ++k) {
             const size_t P = size_t(imgs[k].camera.width) * imgs[k].camera.height;
@@ -348,35 +441,19 @@ TrainerImpl::TrainerImpl(const u3dg_model &initial, const u3dg_image *imgs, int 
                                       stream));
         }
     }
-    dLoss.reserve(maxP * 3);
-    abc.reserve(maxP * 9);
-    dStats.reserve(1, true);
     hStats.reserve(1);
     U3DG_CUDA(cudaMemsetAsync(dStats.p, 0, sizeof(DevStats), stream));
     std::memset(hStats.p, 0, sizeof(DevStats));
-    hCounts.reserve(4);
     statusSlots.reserve(kSlots);
     uniformViews = !cams.empty();
     for (const u3dg_camera &c : cams)
         uniformViews = uniformViews && c.width == cams[0].width && c.height == cams[0].height;
-    descDev.reserve(kGraphSteps, true);
     descHost.reserve(2 * kGraphSteps);
-    statusDev.reserve(kGraphSteps, true);
     graphStatus.reserve(2 * kGraphSteps);
     for (cudaEvent_t &e : chunkDone)
         U3DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    // Intersection buffers sized for 16 tiles per Gaussian at the capacity; they grow on demand.
-    ws.reserveIntersections(std::max<size_t>(size_t(1) << 20, 16 * cap));
-    // Everything a step or a densification needs, at the capacity: no allocation during a schedule
-    // (allocations wait for the device, and pinned ones can take far longer).
-    ws.reserveGaussians(cap);
-    for (DevBuf<int> *b : {&keep, &cost, &costScan, &accCost, &accScan, &isSplit, &splitScan, &keepScan})
-        b->reserve(cap + 1);
-    firstSecond.reserve(2);
-    dScanPartial.reserve(scanPartialEntries(int(cap)) + 1);
     hCounts.reserve(4);
     hNormals.reserve(6 * cap);
-    normals.reserve(6 * cap);
     if (backgroundUpload && count > 0)
         startUploads(imgs, count);
     // The model's host buffers may be released after this call returns (and the images' too, unless

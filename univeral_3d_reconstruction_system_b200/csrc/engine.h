@@ -67,11 +67,14 @@ int guardedCall(F &&f)
 unsigned long long allocEpoch();
 void bumpAllocEpoch();
 
-// Device array with capacity growth (cudaMalloc only when it has to grow).
+// Device array with capacity growth (cudaMalloc only when it has to grow). A buffer may instead hold a
+// slice of a DeviceSlab (owned false): the slab frees it, and a growth past the slice moves the buffer
+// to an allocation of its own.
 template <class T>
 struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;
+    bool owned = true;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
@@ -79,11 +82,22 @@ struct DevBuf {
     void release()
     {
         if (p) {
-            cudaFree(p);
+            if (owned)
+                cudaFree(p);
             bumpAllocEpoch();
         }
         p = nullptr;
         cap = 0;
+        owned = true;
+    }
+    // Takes n elements at mem, which the caller keeps alive (a slab slice).
+    void adopt(void *mem, size_t n)
+    {
+        release();
+        p = static_cast<T *>(mem);
+        cap = n;
+        owned = false;
+        bumpAllocEpoch();
     }
     // Ensures room for n elements; contents are NOT preserved when it grows.
     void reserve(size_t n, bool exact = false)
@@ -104,6 +118,44 @@ struct DevBuf {
         cap = c;
         bumpAllocEpoch();
     }
+};
+
+// One device allocation carved into many buffers. A cudaMalloc that has to map new device memory costs
+// about 0.3 ms whatever its size, so a trainer plans its ~40 buffers (add) and allocates them together
+// (commit) instead of paying that once per buffer. Slices start on 256-byte boundaries. The slab must
+// outlive the buffers' use of their slices (declare it before them).
+class DeviceSlab {
+  public:
+    DeviceSlab() = default;
+    DeviceSlab(const DeviceSlab &) = delete;
+    DeviceSlab &operator=(const DeviceSlab &) = delete;
+    ~DeviceSlab()
+    {
+        for (void *b : bases)
+            cudaFree(b);
+    }
+    // Plans n elements for b (nothing if b already holds that many).
+    template <class T>
+    void add(DevBuf<T> &b, size_t n)
+    {
+        n = std::max<size_t>(n, 1);
+        if (b.p && b.cap >= n)
+            return;
+        items.push_back({&b, n * sizeof(T), n, [](void *buf, void *mem, size_t k) { static_cast<DevBuf<T> *>(buf)->adopt(mem, k); }});
+    }
+    // Allocates everything planned since the last commit and hands out the slices.
+    void commit();
+    size_t bytes() const { return total; }
+
+  private:
+    struct Item {
+        void *buf;
+        size_t bytes, count;
+        void (*adopt)(void *, void *, size_t);
+    };
+    std::vector<Item> items;
+    std::vector<void *> bases;
+    size_t total = 0;
 };
 
 // Pinned host array (for asynchronous device->host reads).
@@ -182,6 +234,11 @@ struct RasterWorkspace {
     void reserveIntersections(size_t capacity);
     // Sizes the per-Gaussian buffers for `count` Gaussians (project() grows them on demand otherwise).
     void reserveGaussians(size_t count);
+    // The same sizes (and the per-pixel buffers for views of up to `pixels` pixels and `tiles` tiles at
+    // the tile size st.tile_size), planned into a slab instead of allocated one by one.
+    void planIntersections(DeviceSlab &slab, size_t capacity);
+    void planGaussians(DeviceSlab &slab, size_t count);
+    void planPixels(DeviceSlab &slab, size_t pixels, int tilesX, int tilesY, int tileSize);
     // Clears the overflow / abort record (stream-ordered).
     void clearCounts(cudaStream_t stream);
     // desc (may be null): the camera of a graph-captured step (see StepDesc).
@@ -208,6 +265,14 @@ struct RasterWorkspace {
     void backwardComposite(const float *dLdRgb, cudaStream_t stream);
     RasterArgs rasterArgs() const;
     ChainArgs chainArgs(const Params &P) const;
+
+  private:
+    // Calls f(buffer, elements) for every per-Gaussian / per-intersection buffer at the given size.
+    template <class F>
+    void eachGaussianBuffer(size_t nn, F &&f);
+    template <class F>
+    void eachIntersectionBuffer(size_t capacity, F &&f);
+    static size_t checkedIntersections(size_t capacity);
 };
 
 // CUDA events around the phases of a profiled step.
@@ -306,6 +371,7 @@ struct TrainerImpl {
     size_t cap = 0;
     int n = 0;
     int cur = 0;                      // which arena holds the live model
+    DeviceSlab slab;                  // the buffers sized at creation (declared first: freed last)
     DevBuf<float> arena[2];           // params, m, v: 3 * 14 * cap floats each
     DevBuf<float> gradAccum;
     DevBuf<int> gradCount;

@@ -13,7 +13,8 @@
 // Compiled with -fmad=false: the contribution decisions (power, alpha, the transmittance cut-off) and
 // the transmittance round exactly like the reference's, so the same entries contribute. The colour
 // sums alone use explicit fused multiply-adds (within 1e-7 of the unfused sums; images are compared
-// within 1e-5).
+// within 1e-5). A thread's two pixels are blended together in sm_100's paired FP32 instructions
+// (add2rn / mul2rn / fma2rn, raster_common.cuh), which round each lane like the scalar operation.
 
 #include "raster_common.cuh"
 
@@ -22,33 +23,6 @@
 namespace u3dg {
 
 namespace {
-
-// One front-to-back blending step of Rasterizer.cpp:305-318 for one pixel.
-__device__ __forceinline__ void blend(const float4 &P, const float4 &Q, const float4 *sR, int j, const ColumnTerms &ct,
-                                      float fy, float minA, float minT, int lastIdx, float &T, float &cr, float &cg,
-                                      float &cb, int &last, bool &done)
-{
-    const float dy = P.y - fy;
-    const float power = powerAt(Q, ct, dy);
-    if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
-        return;
-    const float raw = Q.w * rasterExp(power);
-    const float al = (raw < kMaxAlpha) ? raw : kMaxAlpha;
-    if (al < minA)
-        return;
-    const float nextT = T * (1.0f - al);
-    if (nextT < minT) {
-        done = true;
-        return;
-    }
-    const float w = al * T;
-    const float4 R = sR[j];
-    cr = __fmaf_rn(R.x, w, cr);
-    cg = __fmaf_rn(R.y, w, cg);
-    cb = __fmaf_rn(R.z, w, cb);
-    T = nextT;
-    last = lastIdx;
-}
 
 template <int PB, int BD>
 __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by, float *rgb, float *finalT,
@@ -63,10 +37,10 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
     const int start = a.tileOffsets[tile], end = a.tileOffsets[tile + 1];
     const bool in0 = wb.px < a.width && wb.py0 < a.height, in1 = wb.px < a.width && wb.py1 < a.height;
     bool done0 = !in0, done1 = !in1;
-    float T0 = 1.0f, r0 = 0.0f, g0 = 0.0f, b0c = 0.0f;
-    float T1 = 1.0f, r1 = 0.0f, g1 = 0.0f, b1c = 0.0f;
+    float2 T = make_float2(1.0f, 1.0f), cr = make_float2(0.0f, 0.0f), cg = cr, cb = cr;
     int last0 = 0, last1 = 0;
     const float fx = float(wb.px), fy0 = float(wb.py0), fy1 = float(wb.py1);
+    const float2 one = make_float2(1.0f, 1.0f);
     const float minA = a.minAlpha, minT = a.minTransmittance;
     const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
     for (int b0 = start; b0 < end; b0 += NB) {
@@ -83,18 +57,56 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
             while (bits) {
                 const int j = 32 * k + __ffs(bits) - 1;
                 bits &= bits - 1;
+                // One front-to-back blending step of Rasterizer.cpp:305-318 for both of the thread's
+                // pixels at once: the falloff exponents in scalar (powerAt), then alpha, 1 - alpha,
+                // T (1 - alpha) and alpha T in paired FP32 instructions (each lane rounded like the
+                // scalar operation; none is a product feeding a sum) and the colour sums as paired
+                // fused multiply-adds; the cut-offs per pixel.
                 const float4 P = sP[j], Q = sQ[j];
                 const ColumnTerms ct = columnTerms(Q, P.x - fx);
-                const int idx = b0 - start + j + 1;
-                if (!done0)
-                    blend(P, Q, sR, j, ct, fy0, minA, minT, idx, T0, r0, g0, b0c, last0, done0);
-                if (!done1)
-                    blend(P, Q, sR, j, ct, fy1, minA, minT, idx, T1, r1, g1, b1c, last1, done1);
+                const float2 pw = make_float2(powerAt(Q, ct, P.y - fy0), powerAt(Q, ct, P.y - fy1));
+                bool v0 = !done0 && !(pw.x > 0.0f || pw.x < P.z);
+                bool v1 = !done1 && !(pw.y > 0.0f || pw.y < P.z);
+                if (v0 || v1) {
+                    // A pixel that is out gets exp(0), whose alpha it never uses.
+                    const float2 G = make_float2(rasterExp(v0 ? pw.x : 0.0f), rasterExp(v1 ? pw.y : 0.0f));
+                    const float2 raw = mul2rn(make_float2(Q.w, Q.w), G);
+                    const float al0 = (raw.x < kMaxAlpha) ? raw.x : kMaxAlpha;
+                    const float al1 = (raw.y < kMaxAlpha) ? raw.y : kMaxAlpha;
+                    v0 = v0 && !(al0 < minA);
+                    v1 = v1 && !(al1 < minA);
+                    const float2 nT = mul2rn(T, add2rn(one, make_float2(-al0, -al1)));
+                    if (v0 && nT.x < minT) {
+                        done0 = true;
+                        v0 = false;
+                    }
+                    if (v1 && nT.y < minT) {
+                        done1 = true;
+                        v1 = false;
+                    }
+                    float2 w = mul2rn(make_float2(al0, al1), T);
+                    w.x = v0 ? w.x : 0.0f; // a pixel that does not blend adds R * 0 = 0 to its sums
+                    w.y = v1 ? w.y : 0.0f;
+                    const float4 R = sR[j];
+                    cr = fma2rn(make_float2(R.x, R.x), w, cr);
+                    cg = fma2rn(make_float2(R.y, R.y), w, cg);
+                    cb = fma2rn(make_float2(R.z, R.z), w, cb);
+                    const int idx = b0 - start + j + 1;
+                    if (v0) {
+                        T.x = nT.x;
+                        last0 = idx;
+                    }
+                    if (v1) {
+                        T.y = nT.y;
+                        last1 = idx;
+                    }
+                }
                 if (done0 && done1)
                     break;
             }
         }
     }
+    const float T0 = T.x, T1 = T.y, r0 = cr.x, r1 = cr.y, g0 = cg.x, g1 = cg.y, b0c = cb.x, b1c = cb.y;
     if (in0) {
         const size_t pix = size_t(wb.py0) * a.width + wb.px;
         rgb[pix * 3] = r0 + T0 * a.bg[0];

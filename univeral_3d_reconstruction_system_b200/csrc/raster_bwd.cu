@@ -18,6 +18,10 @@
 // tolerance). The recovery keeps the correctly rounded division: an approximate division (2 ulp) or a
 // reciprocal-multiply made the backward 3 % faster but moved some colour gradients just past 1e-4
 // relative to the reference's.
+//
+// A thread's two pixels are replayed together: the falloff exponents and the divisions in scalar, the
+// rest of each step in paired FP32 instructions (raster_common.cuh), one float2 lane per pixel. A
+// pixel that does not contribute at an entry keeps its state (selects) and adds zero to the sums.
 
 #include "raster_common.cuh"
 
@@ -29,68 +33,21 @@ namespace u3dg {
 
 namespace {
 
-// Per-pixel state of the back-to-front replay. The colour behind the current entry enters the
-// gradient only through its dot product with dL/dpixel, so the state keeps that scalar (accd, the
-// running sum over channels of accum[ch] * dpix[ch]) and the last entry's colour dot product (lcd)
-// instead of three channels each: the recurrence accum = lastAlpha * lastColour + (1 - lastAlpha) *
-// accum is linear, so accd follows the same recurrence on the dot products. Three fewer multiply-adds
-// per channel per pair and eight fewer live registers for a thread's two pixels (no spills); the sums
-// differ from the per-channel form by rounding only (within the gradient tolerance).
-struct PixelState {
-    float T, accd, lcd, lastAlpha;
-    float fT, d0, d1, d2, bgDot, fy;
-    int nC;
+// Back-to-front replay state of a thread's two pixels (one float2 lane each). The colour behind the
+// current entry enters the gradient only through its dot product with dL/dpixel, so the state keeps
+// that scalar (the running sum over channels of accum[ch] * dpix[ch], kept negated: nacc) and the last
+// contributor's colour dot product (lcd) instead of three channels each: the recurrence accum =
+// lastAlpha * lastColour + (1 - lastAlpha) * accum is linear, so the dot products follow it too (the
+// sums differ from the per-channel form by rounding only, within the gradient tolerance). lastAlpha is
+// kept negated as well (nla), so every update is a paired add or fused multiply-add.
+struct PixelPair {
+    float2 T, nacc, lcd, nla; // transmittance, -(colour dot behind), last contributor's colour dot, -its alpha
+    float2 d0, d1, d2, fy;    // dL/dpixel per channel, pixel row
+    float2 fT, bgDot;         // final transmittance, background . dL/dpixel (background term only)
+    int nC0, nC1;             // contributor counts
 };
 
-// One back-to-front step of Rasterizer.cpp:385-416 for one pixel; adds its 9 contributions to c.
-// kBg: the background is not black (its term enters dAlpha).
-template <bool kBg>
-__device__ __forceinline__ bool pairGrad(const float4 &P, const float4 &Q, const float4 *sR, int jj, float dx,
-                                         const ColumnTerms &ct, float minA, PixelState &s, float c[kG2d])
-{
-    const float dy = __fsub_rn(P.y, s.fy);
-    const float power = powerAt(Q, ct, dy);
-    if (power > 0.0f || power < P.z) // P.z: SplatRec::powMin
-        return false;
-    const float G = rasterExp(power);
-    const float raw = __fmul_rn(Q.w, G);
-    const float al = (raw < kMaxAlpha) ? raw : kMaxAlpha;
-    if (al < minA)
-        return false;
-    const float4 R = sR[jj];
-    s.T = __fdiv_rn(s.T, __fsub_rn(1.0f, al));
-    const float w = al * s.T;
-    // dAlpha = sum_ch (colour[ch] - accum[ch]) * dpix[ch] * T (Rasterizer.cpp:393-399), on dot products.
-    const float rd = R.x * s.d0 + R.y * s.d1 + R.z * s.d2;
-    s.accd = s.accd + s.lastAlpha * (s.lcd - s.accd); // lastAlpha * lcd + (1 - lastAlpha) * accd
-    s.lcd = rd;
-    float dAl = (rd - s.accd) * s.T;
-    c[5] += w * s.d0;
-    c[6] += w * s.d1;
-    c[7] += w * s.d2;
-    s.lastAlpha = al;
-    // -finalT / (1 - alpha) * bgDot: with a black background (kBg false) it would add a signed zero,
-    // which leaves dAl unchanged, so those launches compile it out.
-    if (kBg)
-        dAl += -s.fT / (1.0f - al) * s.bgDot;
-    if (raw > kMaxAlpha)
-        return true; // clamped alpha: colour gradient only
-    const float t = G * dAl;
-    c[8] += t;
-    // The mean and conic gradients are linear in the per-pixel moments of dPow: sum dPow dx, dPow dy,
-    // dPow dx^2, dPow dx dy, dPow dy^2, and combine them with the conic once per list entry
-    // (finishEntry) instead of once per pixel. A thread's two pixels share dx, so the pixels add
-    // sum dPow (c[0]), dPow dy (c[1]) and dPow dy^2 (c[4]) only; the thread multiplies by dx once
-    // (c[0] -> dx sum dPow, c[2] = dx^2 sum dPow, c[3] = dx sum dPow dy) before the warp sum.
-    const float dPow = Q.w * t;
-    const float pdy = dPow * dy;
-    c[0] += dPow;
-    c[1] += pdy;
-    c[4] += pdy * dy;
-    return true;
-}
-
-// Turns an entry's summed moments (pairGrad) into dL/dmean2d and dL/dconic (Rasterizer.cpp:405-412):
+// Turns an entry's summed moments (the entry loop) into dL/dmean2d and dL/dconic (Rasterizer.cpp:405-412):
 // dmean = -(A m_x + B m_y, C m_y + B m_x), dA = -m_xx / 2, dB = -m_xy, dC = -m_yy / 2.
 __device__ __forceinline__ void finishEntry(const float4 &Q, float g[kG2d])
 {
@@ -137,18 +94,22 @@ __device__ __forceinline__ float warpReduce9(const float c[kG2d], int lane, floa
     return v;
 }
 
-__device__ __forceinline__ void initPixel(PixelState &s, bool inside, size_t pix, float fy, const float *dLdRgb,
-                                          const float *finalT, const int *nContrib, const float *bg)
+__device__ __forceinline__ PixelPair initPair(bool in0, bool in1, size_t pix0, size_t pix1, float fy0, float fy1,
+                                              const float *dLdRgb, const float *finalT, const int *nContrib,
+                                              const float *bg)
 {
-    s.nC = inside ? nContrib[pix] : 0;
-    s.fT = inside ? finalT[pix] : 0.0f;
-    s.d0 = inside ? dLdRgb[pix * 3] : 0.0f;
-    s.d1 = inside ? dLdRgb[pix * 3 + 1] : 0.0f;
-    s.d2 = inside ? dLdRgb[pix * 3 + 2] : 0.0f;
-    s.bgDot = bg[0] * s.d0 + bg[1] * s.d1 + bg[2] * s.d2;
-    s.T = s.fT;
-    s.accd = s.lcd = s.lastAlpha = 0.0f;
-    s.fy = fy;
+    PixelPair p;
+    p.nC0 = in0 ? nContrib[pix0] : 0;
+    p.nC1 = in1 ? nContrib[pix1] : 0;
+    p.fT = make_float2(in0 ? finalT[pix0] : 0.0f, in1 ? finalT[pix1] : 0.0f);
+    p.d0 = make_float2(in0 ? dLdRgb[pix0 * 3] : 0.0f, in1 ? dLdRgb[pix1 * 3] : 0.0f);
+    p.d1 = make_float2(in0 ? dLdRgb[pix0 * 3 + 1] : 0.0f, in1 ? dLdRgb[pix1 * 3 + 1] : 0.0f);
+    p.d2 = make_float2(in0 ? dLdRgb[pix0 * 3 + 2] : 0.0f, in1 ? dLdRgb[pix1 * 3 + 2] : 0.0f);
+    p.bgDot = make_float2(bg[0] * p.d0.x + bg[1] * p.d1.x + bg[2] * p.d2.x, bg[0] * p.d0.y + bg[1] * p.d1.y + bg[2] * p.d2.y);
+    p.T = p.fT;
+    p.nacc = p.lcd = p.nla = make_float2(0.0f, 0.0f);
+    p.fy = make_float2(fy0, fy1);
+    return p;
 }
 
 template <int PB, int BD, bool kBg>
@@ -168,9 +129,10 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
         const int per = a.tileSize / PB;
         partial += size_t((by % per) * per + bx % per) * a.subStride;
     }
-    PixelState s0, s1;
-    initPixel(s0, in0, in0 ? size_t(wb.py0) * a.width + wb.px : 0, float(wb.py0), dLdRgb, finalTIn, nContribIn, a.bg);
-    initPixel(s1, in1, in1 ? size_t(wb.py1) * a.width + wb.px : 0, float(wb.py1), dLdRgb, finalTIn, nContribIn, a.bg);
+    PixelPair pp = initPair(in0, in1, in0 ? size_t(wb.py0) * a.width + wb.px : 0,
+                            in1 ? size_t(wb.py1) * a.width + wb.px : 0, float(wb.py0), float(wb.py1), dLdRgb,
+                            finalTIn, nContribIn, a.bg);
+    const float2 one2 = make_float2(1.0f, 1.0f);
     const float fx = float(wb.px);
     const float minA = a.minAlpha;
     const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
@@ -178,7 +140,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     if (tid == 0)
         sMax = 0;
     __syncthreads();
-    const int nMax = max(s0.nC, s1.nC);
+    const int nMax = max(pp.nC0, pp.nC1);
     if (nMax > 0)
         atomicMax(&sMax, nMax);
     // This warp's pixels have no contributor at or beyond wMax: the warp skips those entries.
@@ -226,17 +188,68 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                 for (int q = 0; q < kG2d; ++q)
                     c[q] = 0.0f;
                 bool act = false;
-                if (j < s0.nC || j < s1.nC) {
+                if (j < pp.nC0 || j < pp.nC1) {
                     const float4 P = sP[jj], Q = sQ[jj];
                     const float dx = __fsub_rn(P.x, fx);
                     const ColumnTerms ct = columnTerms(Q, dx);
-                    if (j < s0.nC)
-                        act |= pairGrad<kBg>(P, Q, sR, jj, dx, ct, minA, s0, c);
-                    if (j < s1.nC)
-                        act |= pairGrad<kBg>(P, Q, sR, jj, dx, ct, minA, s1, c);
-                    c[3] = dx * c[1];
-                    c[0] = dx * c[0];
-                    c[2] = dx * c[0]; // c[0] already holds dx sum dPow
+                    // Falloff exponents in scalar, exactly as the forward decides (powerAt).
+                    const float2 dy = make_float2(__fsub_rn(P.y, pp.fy.x), __fsub_rn(P.y, pp.fy.y));
+                    const float2 pw = make_float2(powerAt(Q, ct, dy.x), powerAt(Q, ct, dy.y));
+                    bool v0 = j < pp.nC0 && !(pw.x > 0.0f || pw.x < P.z);
+                    bool v1 = j < pp.nC1 && !(pw.y > 0.0f || pw.y < P.z);
+                    if (v0 || v1) {
+                        // One back-to-front step of Rasterizer.cpp:385-416 for both pixels (a pixel that
+                        // is out gets exp(0) and zero weights, and keeps its state).
+                        const float2 G = make_float2(rasterExp(v0 ? pw.x : 0.0f), rasterExp(v1 ? pw.y : 0.0f));
+                        const float2 raw = mul2rn(make_float2(Q.w, Q.w), G);
+                        const float al0 = (raw.x < kMaxAlpha) ? raw.x : kMaxAlpha;
+                        const float al1 = (raw.y < kMaxAlpha) ? raw.y : kMaxAlpha;
+                        v0 = v0 && !(al0 < minA);
+                        v1 = v1 && !(al1 < minA);
+                        if (v0 || v1) {
+                            act = true;
+                            const float4 R = sR[jj];
+                            // Transmittance before this entry: T / (1 - alpha), correctly rounded.
+                            const float2 om = add2rn(one2, make_float2(-al0, -al1));
+                            const float Tn0 = __fdiv_rn(pp.T.x, om.x), Tn1 = __fdiv_rn(pp.T.y, om.y);
+                            pp.T = make_float2(v0 ? Tn0 : pp.T.x, v1 ? Tn1 : pp.T.y);
+                            const float2 w = mul2rn(make_float2(v0 ? al0 : 0.0f, v1 ? al1 : 0.0f), pp.T);
+                            // dAlpha = (colour . dpix - accum . dpix) T (Rasterizer.cpp:393-399), on the
+                            // dot products; accum takes the previous contributor's colour first.
+                            const float2 rd = fma2rn(make_float2(R.z, R.z), pp.d2,
+                                                         fma2rn(make_float2(R.y, R.y), pp.d1,
+                                                                    mul2rn(make_float2(R.x, R.x), pp.d0)));
+                            const float2 nacc = fma2rn(pp.nla, add2rn(pp.lcd, pp.nacc), pp.nacc);
+                            float2 dAl = mul2rn(add2rn(rd, nacc), pp.T);
+                            pp.nacc = make_float2(v0 ? nacc.x : pp.nacc.x, v1 ? nacc.y : pp.nacc.y);
+                            pp.lcd = make_float2(v0 ? rd.x : pp.lcd.x, v1 ? rd.y : pp.lcd.y);
+                            pp.nla = make_float2(v0 ? -al0 : pp.nla.x, v1 ? -al1 : pp.nla.y);
+                            const float2 wd0 = mul2rn(w, pp.d0), wd1 = mul2rn(w, pp.d1), wd2 = mul2rn(w, pp.d2);
+                            c[5] = wd0.x + wd0.y;
+                            c[6] = wd1.x + wd1.y;
+                            c[7] = wd2.x + wd2.y;
+                            if (kBg) {
+                                dAl.x += -pp.fT.x / om.x * pp.bgDot.x;
+                                dAl.y += -pp.fT.y / om.y * pp.bgDot.y;
+                            }
+                            // A clamped alpha has a colour gradient only.
+                            const bool m0 = v0 && !(raw.x > kMaxAlpha), m1 = v1 && !(raw.y > kMaxAlpha);
+                            float2 t = mul2rn(G, dAl);
+                            t = make_float2(m0 ? t.x : 0.0f, m1 ? t.y : 0.0f);
+                            c[8] = t.x + t.y;
+                            // The mean and conic gradients are linear in the per-pixel moments of dPow
+                            // (finishEntry combines them with the conic once per entry); both pixels
+                            // share dx, so dx multiplies the thread's sums once.
+                            const float2 dPow = mul2rn(make_float2(Q.w, Q.w), t);
+                            const float2 pdy = mul2rn(dPow, dy);
+                            const float2 pdyy = mul2rn(pdy, dy);
+                            c[1] = pdy.x + pdy.y;
+                            c[4] = pdyy.x + pdyy.y;
+                            c[0] = dx * (dPow.x + dPow.y);
+                            c[2] = dx * c[0];
+                            c[3] = dx * c[1];
+                        }
+                    }
                 }
                 if (__any_sync(0xffffffffu, act)) {
                     float v8;

@@ -168,4 +168,45 @@ __device__ __forceinline__ float powerAt(const float4 &Q, const ColumnTerms &c, 
 
 __device__ __forceinline__ float rasterExp(float x) { return expf(x); }
 
+// Paired FP32 arithmetic (sm_100: one instruction computes two float lanes), each lane rounded like
+// the scalar __fmul_rn / __fadd_rn / __fmaf_rn. One caveat, measured with CUDA 12.9: a paired add
+// whose operand is a paired product is fused into a single rounding by the code generator (for the
+// float2 intrinsics, for these explicit .rn instructions, and with -fmad=false alike: on random inputs
+// a + (z d) d came out fused in 23 % of the cases). So arithmetic that decides which pairs contribute
+// (the falloff exponent) stays scalar, and paired instructions take only steps that have no product
+// feeding a sum, or whose rounding is free (gradient arithmetic, colour sums).
+__device__ __forceinline__ float2 mul2rn(float2 a, float2 b)
+{
+    float2 d;
+    asm("{ .reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd; }"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 add2rn(float2 a, float2 b)
+{
+    float2 d;
+    asm("{ .reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd; }"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// a * b + c per lane with one rounding (fma.rn.f32x2).
+__device__ __forceinline__ float2 fma2rn(float2 a, float2 b, float2 c)
+{
+    float2 d;
+    asm("{ .reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd; }"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 } // namespace u3dg
