@@ -58,13 +58,17 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
                 const int j = 32 * k + __ffs(bits) - 1;
                 bits &= bits - 1;
                 // One front-to-back blending step of Rasterizer.cpp:305-318 for both of the thread's
-                // pixels at once: the falloff exponents in scalar (powerAt), then alpha, 1 - alpha,
-                // T (1 - alpha) and alpha T in paired FP32 instructions (each lane rounded like the
-                // scalar operation; none is a product feeding a sum) and the colour sums as paired
-                // fused multiply-adds; the cut-offs per pixel.
+                // pixels at once, in paired FP32 instructions where each lane rounds like the scalar
+                // operation: the falloff exponent in powerAt's order (products paired, sums scalar),
+                // alpha, 1 - alpha, T (1 - alpha) and alpha T, and the colour sums as paired fused
+                // multiply-adds; the cut-offs per pixel.
                 const float4 P = sP[j], Q = sQ[j];
                 const ColumnTerms ct = columnTerms(Q, P.x - fx);
-                const float2 pw = make_float2(powerAt(Q, ct, P.y - fy0), powerAt(Q, ct, P.y - fy1));
+                const float2 dy = make_float2(P.y - fy0, P.y - fy1);
+                const float2 cdd = mul2rn(mul2rn(make_float2(Q.z, Q.z), dy), dy);
+                const float2 bdy = mul2rn(make_float2(ct.bx, ct.bx), dy);
+                const float2 hq = mul2rn(make_float2(-0.5f, -0.5f), make_float2(__fadd_rn(ct.axx, cdd.x), __fadd_rn(ct.axx, cdd.y)));
+                const float2 pw = make_float2(__fsub_rn(hq.x, bdy.x), __fsub_rn(hq.y, bdy.y));
                 bool v0 = !done0 && !(pw.x > 0.0f || pw.x < P.z);
                 bool v1 = !done1 && !(pw.y > 0.0f || pw.y < P.z);
                 if (v0 || v1) {

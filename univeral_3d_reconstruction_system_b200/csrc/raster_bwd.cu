@@ -19,9 +19,9 @@
 // reciprocal-multiply made the backward 3 % faster but moved some colour gradients just past 1e-4
 // relative to the reference's.
 //
-// A thread's two pixels are replayed together: the falloff exponents and the divisions in scalar, the
-// rest of each step in paired FP32 instructions (raster_common.cuh), one float2 lane per pixel. A
-// pixel that does not contribute at an entry keeps its state (selects) and adds zero to the sums.
+// A thread's two pixels are replayed together in paired FP32 instructions (raster_common.cuh), one
+// float2 lane per pixel; the falloff exponents' sums and the divisions stay scalar. A pixel that does
+// not contribute at an entry keeps its state (selects) and adds zero to the sums.
 
 #include "raster_common.cuh"
 
@@ -192,9 +192,13 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                     const float4 P = sP[jj], Q = sQ[jj];
                     const float dx = __fsub_rn(P.x, fx);
                     const ColumnTerms ct = columnTerms(Q, dx);
-                    // Falloff exponents in scalar, exactly as the forward decides (powerAt).
+                    // Falloff exponents exactly as the forward decides (powerAt's order; products
+                    // paired, sums scalar).
                     const float2 dy = make_float2(__fsub_rn(P.y, pp.fy.x), __fsub_rn(P.y, pp.fy.y));
-                    const float2 pw = make_float2(powerAt(Q, ct, dy.x), powerAt(Q, ct, dy.y));
+                    const float2 cdd = mul2rn(mul2rn(make_float2(Q.z, Q.z), dy), dy);
+                    const float2 bdy = mul2rn(make_float2(ct.bx, ct.bx), dy);
+                    const float2 hq = mul2rn(make_float2(-0.5f, -0.5f), make_float2(__fadd_rn(ct.axx, cdd.x), __fadd_rn(ct.axx, cdd.y)));
+                    const float2 pw = make_float2(__fsub_rn(hq.x, bdy.x), __fsub_rn(hq.y, bdy.y));
                     bool v0 = j < pp.nC0 && !(pw.x > 0.0f || pw.x < P.z);
                     bool v1 = j < pp.nC1 && !(pw.y > 0.0f || pw.y < P.z);
                     if (v0 || v1) {

@@ -172,9 +172,11 @@ __device__ __forceinline__ float rasterExp(float x) { return expf(x); }
 // the scalar __fmul_rn / __fadd_rn / __fmaf_rn. One caveat, measured with CUDA 12.9: a paired add
 // whose operand is a paired product is fused into a single rounding by the code generator (for the
 // float2 intrinsics, for these explicit .rn instructions, and with -fmad=false alike: on random inputs
-// a + (z d) d came out fused in 23 % of the cases). So arithmetic that decides which pairs contribute
-// (the falloff exponent) stays scalar, and paired instructions take only steps that have no product
-// feeding a sum, or whose rounding is free (gradient arithmetic, colour sums).
+// a + (z d) d came out fused in 23 % of the cases). So in arithmetic that decides which pairs
+// contribute (the falloff exponent) the products are paired and the sums scalar (a scalar add of a
+// lane of a paired product rounded separately in all of 3e8 random cases), and elsewhere paired
+// instructions take only steps that have no product feeding a sum, or whose rounding is free
+// (gradient arithmetic, colour sums).
 __device__ __forceinline__ float2 mul2rn(float2 a, float2 b)
 {
     float2 d;
