@@ -3,8 +3,11 @@
 Workload "high-300k": the High preset scene (250k ground-truth Gaussians with SH degree 3, 150 views at
 640x480 on a hemisphere with random roll, seed 0) and a model at the preset's 300k-Gaussian cap
 (initGaussiansFromPoints of every true centre plus 50k noisy re-samples). A step is one
-Trainer::step (forward, L1 + D-SSIM loss, backward, Adam) on the next view of the shuffled order, with
-densification finished (the steady phase after refine_stop of the 7000-iteration schedule).
+Trainer::step (forward, L1 + D-SSIM loss, backward, Adam) on the next view of the shuffled order, at a
+fixed model size: no densification or opacity reset (as after refine_stop of the 7000-iteration
+schedule). The timed steps follow W warm-up steps from the initialisation, whose low opacities (0.1)
+let every pixel run through more of its list than a trained model does: a 20-step run after 5 warm-up
+steps costs about 15 % more per step than steps a few hundred iterations later.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -533,7 +536,8 @@ def config(args, dist: Dist) -> dict:
             "scene": f"{preset} preset (seed 0): {sp.gt_count} GT Gaussians, SH3, {sp.views} views "
                      f"{sp.width}x{sp.height}",
             "model_gaussians": cap, "resolution": f"{sp.width}x{sp.height}", "views": sp.views, "tile": 16,
-            "phase": "steady (densification finished)", "parallelism": f"replicas x{dist.world}",
+            "phase": f"fixed size (no densification or reset), steps {args.warmup}..{args.warmup + args.steps} "
+                     "after initGaussiansFromPoints", "parallelism": f"replicas x{dist.world}",
             "l2": "inputs larger than L2: per step the model, Adam moments and raster buffers (~0.3 GB) "
                   "exceed the 126 MB L2"}
 
