@@ -335,7 +335,7 @@ int u3dg_photometric_loss(const float *render, const float *target, int width, i
 int u3dg_psnr(const float *a, const float *b, size_t count, float *out);
 /* No reference counterpart: u3dg_photometric_loss on DEVICE pointers (render, target, grad are
  * height*width*3 floats in device memory of the current device) that allocates nothing. Temporaries
- * live in a fixed 11.1 MB device array per device, so width*height must be <= 640*480 and the image
+ * live in a fixed 11.2 MB device array per device, so width*height must be <= 640*480 and the image
  * at most 2048 loss blocks of 32x16 pixels; larger images return U3DG_ERR_CAPACITY. Work runs on
  * `stream` (a cudaStream_t; NULL = the default stream), and the call synchronises it before
  * returning (it returns the loss values on the host). The first call in each device context (the

@@ -10,10 +10,11 @@
 // Within a tile the emission order, i.e. (depth bits, id), survives, which is exactly the
 // reference's list.
 //
-// The intersection count is only known on the device, so nothing here waits for the host: item
-// counts are read from device memory, grids are sized for the capacity, and a capacity check turns
-// an overflow into an empty bin list plus a flag the host reads later (it then grows the buffers and
-// replays the step).
+// The intersection count is only known on the device, so nothing here waits for the host: the tile
+// sort reads its item count from device memory (the depth sort takes the host-known Gaussian count),
+// grids are sized for the capacity, and a capacity check (in the scan of the per-rank tile counts)
+// turns an overflow into an empty bin list plus a flag the host reads later (it then grows the
+// buffers and replays the step).
 //
 // Sorting: stable LSD passes, 8-bit digits for the depth keys and one 11-bit pass for tile ids (up to
 // 2048 tiles; that pass's scatter also writes the tile lists' Gaussian ids and, in block 0, the tile
@@ -86,8 +87,8 @@ __device__ __forceinline__ void chunkOf(int n, int G, int b, int &begin, int &en
 }
 
 template <int DB>
-__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int shift, int *hist,
-                                                            int G)
+__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int nHost, int shift,
+                                                            int *hist, int G)
 {
     pdlEntry();
     constexpr int R = 1 << DB;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys
         counts[d] = 0;
     __syncthreads();
     int begin, end;
-    chunkOf(*nPtr, G, blockIdx.x, begin, end);
+    chunkOf(nPtr ? *nPtr : nHost, G, blockIdx.x, begin, end);
     for (int i = begin + threadIdx.x; i < end; i += kThreads)
         atomicAdd(&counts[(keys[i] >> shift) & uint32_t(R - 1)], 1);
     __syncthreads();
@@ -134,16 +135,17 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G,
 template <int DB, bool kTiles = false>
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
                                                                uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
-                                                               int shift, const int *hist, const int *rowTotals, int G,
-                                                               TileFinish fin)
+                                                               int nHost, int shift, const int *hist, const int *rowTotals,
+                                                               int G, TileFinish fin)
 {
     pdlEntry();
+    const int n = nPtr ? *nPtr : nHost;
     constexpr int R = 1 << DB;
     __shared__ uint8_t warpCounts[kWarps][R];
     __shared__ int base[R];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int begin, end;
-    chunkOf(*nPtr, G, blockIdx.x, begin, end);
+    chunkOf(n, G, blockIdx.x, begin, end);
     for (int k = threadIdx.x; k < kWarps * R; k += kThreads)
         (&warpCounts[0][0])[k] = 0;
     {
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
         for (int d = threadIdx.x; d < fin.tiles; d += kThreads)
             fin.tileOffsets[d] = base[d]; // block 0's row prefix is zero
         if (threadIdx.x == 0)
-            fin.tileOffsets[fin.tiles] = *nPtr;
+            fin.tileOffsets[fin.tiles] = n;
     }
     const uint32_t lanesBelow = (1u << lane) - 1u;
     uint8_t *myCounts = warpCounts[warp];
@@ -224,6 +226,23 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
     }
 }
 
+// Capacity check of a bin pass on its intersection count t: the usable count is t, or 0 when t
+// exceeds the intersection buffers or a previous step already aborted (the abort is sticky until the
+// host clears it). iteration identifies the aborted step for the host.
+__device__ __forceinline__ void checkCapacity(int t, int capacity, BinCounts *c, int iteration, const StepDesc *desc)
+{
+    if (desc)
+        iteration = desc->iteration;
+    const bool over = t < 0 || t > capacity;
+    if (over) {
+        if (c->abortIter < 0)
+            c->abortIter = iteration;
+        c->need = max(c->need, t < 0 ? INT_MAX : t);
+    }
+    c->total = t;
+    c->effTotal = (over || c->abortIter >= 0) ? 0 : t;
+}
+
 // Exclusive scan, reduce-then-scan over a host-known n.
 constexpr int kScanTile = kThreads * 8;
 
@@ -261,7 +280,9 @@ __global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int 
         partial[B] = carry;
 }
 
-__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B)
+// cap.counts (may be null): block 0 also runs the bin pass's capacity check on the total.
+__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B,
+                                                                ScanCapacity cap)
 {
     pdlEntry();
     const int base = blockIdx.x * kScanTile + threadIdx.x * 8;
@@ -280,8 +301,11 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
             out[base + r] = run;
         run += v[r];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         out[n] = partial[B];
+        if (cap.counts != nullptr)
+            checkCapacity(partial[B], cap.capacity, cap.counts, cap.iteration, cap.desc);
+    }
 }
 
 // Tile culling (trainers): a Gaussian is listed only in the tiles of its rectangle that its
@@ -385,23 +409,12 @@ __global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, co
     cnt[r] = c;
 }
 
-// Capacity check of this bin pass: the usable count is the scan total, or 0 when it exceeds the
-// intersection buffers or a previous step already aborted (the abort is sticky until the host
-// clears it). iteration identifies the aborted step for the host.
+// Capacity check of a bin pass on its scan total (checkCapacity), when the scan had no kernels to
+// fold it into.
 __global__ void capacityKernel(const int *total, int capacity, BinCounts *c, int iteration, const StepDesc *desc)
 {
     pdlEntry();
-    if (desc)
-        iteration = desc->iteration;
-    const int t = *total;
-    const bool over = t < 0 || t > capacity;
-    if (over) {
-        if (c->abortIter < 0)
-            c->abortIter = iteration;
-        c->need = max(c->need, t < 0 ? INT_MAX : t);
-    }
-    c->total = t;
-    c->effTotal = (over || c->abortIter >= 0) ? 0 : t;
+    checkCapacity(*total, capacity, c, iteration, desc);
 }
 
 // One warp per 32 consecutive depth ranks (grid-stride): the warp writes its ranks' intersections in
@@ -536,7 +549,7 @@ int radixDigits() { return 1 << kWideBits; }
 
 int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
-                   const TileFinish *fin)
+                   const TileFinish *fin, int nHost)
 {
     uint32_t *kin = keysA, *kout = keysB, *vout = valsB;
     const uint32_t *vin = nullptr;
@@ -550,16 +563,16 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     int passes = 0;
     for (int shift = 0; shift < bits; shift += db, ++passes) {
         if (wide) {
-            { launchPdl(radixHistKernel<kWideBits>, G, kThreads, 0, s, kin, nDev, shift, hist, G); countLaunch(); }
+            { launchPdl(radixHistKernel<kWideBits>, G, kThreads, 0, s, kin, nDev, nHost, shift, hist, G); countLaunch(); }
             { launchPdl(radixRowScanKernel, 1 << kWideBits, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
             if (fin != nullptr)
-                { launchPdl(radixScatterKernel<kWideBits, true>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, *fin); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits, true>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, *fin); countLaunch(); }
             else
-                { launchPdl(radixScatterKernel<kWideBits>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         } else {
-            { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, kin, nDev, shift, hist, G); countLaunch(); }
+            { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, kin, nDev, nHost, shift, hist, G); countLaunch(); }
             { launchPdl(radixRowScanKernel, 1 << 8, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
-            { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+            { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
         }
         uint32_t *nk = kin;
         kin = kout;
@@ -574,16 +587,31 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
 
 size_t scanPartialEntries(int n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
 
-void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
+static void scanLaunches(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s)
 {
     const int B = (n + kScanTile - 1) / kScanTile;
+    { launchPdl(scanReduceKernel, B, kThreads, 0, s, in, n, partial); countLaunch(); }
+    { launchPdl(scanPartialKernel, 1, kThreads, 0, s, partial, B); countLaunch(); }
+    { launchPdl(scanDownsweepKernel, B, kThreads, 0, s, in, out, n, partial, B, cap); countLaunch(); }
+}
+
+void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
+{
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(int), s);
         return;
     }
-    { launchPdl(scanReduceKernel, B, kThreads, 0, s, in, n, partial); countLaunch(); }
-    { launchPdl(scanPartialKernel, 1, kThreads, 0, s, partial, B); countLaunch(); }
-    { launchPdl(scanDownsweepKernel, B, kThreads, 0, s, in, out, n, partial, B); countLaunch(); }
+    scanLaunches(in, out, n, partial, ScanCapacity{0, nullptr, 0, nullptr}, s);
+}
+
+void exclusiveScanChecked(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s)
+{
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, sizeof(int), s);
+        launchCapacityCheck(out, cap.capacity, cap.counts, cap.iteration, s, cap.desc);
+        return;
+    }
+    scanLaunches(in, out, n, partial, cap, s);
 }
 
 size_t cullRowEntries(size_t n) { return n * kCullRows; }
@@ -593,16 +621,6 @@ void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *ra
 {
     if (n > 0)
         { launchPdl(rankCountsKernel, grid(n, 256), 256, 0, s, sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf, rowTab); countLaunch(); }
-}
-
-namespace {
-__global__ void setCountKernel(BinCounts *c, int n) {
-    pdlEntry(); c->n = n; }
-} // namespace
-
-void launchSetCount(BinCounts *c, int n, cudaStream_t s)
-{
-    { launchPdl(setCountKernel, 1, 1, 0, s, c, n); countLaunch(); }
 }
 
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,

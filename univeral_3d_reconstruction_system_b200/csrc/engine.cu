@@ -229,15 +229,13 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     rowTotals.reserve(size_t(radixDigits()));
     tileOffsets.reserve(size_t(tiles) + 1);
     uint32_t *keysOut = nullptr, *valsOut = nullptr;
-    launchSetCount(counts.p, n, stream);
-    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, &counts.p->n, std::max(n, 1), 32, hist.p,
-                   rowTotals.p, &keysOut, &valsOut, stream);
+    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, nullptr, std::max(n, 1), 32, hist.p, rowTotals.p,
+                   &keysOut, &valsOut, stream, nullptr, n);
     sortedIds = valsOut;
     // The emission's row table packs cumulative counts of 8 rows in 16 bits: rows of at most 8191 tiles.
     const SplatRec *cullRec = (cullTiles && tilesX < 8192) ? rec.p : nullptr;
     launchRankCounts(sortedIds, rect.p, radius.p, cullRec, st.tile_size, n, cnt.p, rankOf.p, rowTab.p, stream);
-    exclusiveScan(cnt.p, offs.p, n, scanPartial.p, stream);
-    launchCapacityCheck(offs.p + n, icap, counts.p, iteration, stream, desc);
+    exclusiveScanChecked(cnt.p, offs.p, n, scanPartial.p, ScanCapacity{icap, counts.p, iteration, desc}, stream);
     launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, cullRec, st.tile_size, rowTab.p, iKeys0.p,
                emitGid.p, stream);
     int bits = 0;

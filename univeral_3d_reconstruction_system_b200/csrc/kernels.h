@@ -43,12 +43,11 @@ inline void launchPdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sm
 // Device-side sizes of one bin pass. The host never waits for them inside a step: it reads the
 // struct back asynchronously and checks it one step later.
 struct BinCounts {
-    int n;         // Gaussians in the pass (input of the depth sort)
     int total;     // tile-Gaussian intersections found by the scan
     int effTotal;  // intersections actually binned: total, or 0 after an overflow / abort
     int abortIter; // -1, or the first step whose intersections did not fit (sticky until cleared)
     int need;      // largest intersection count that did not fit
-    int pad[3];
+    int pad[4];
 };
 
 // The values of one training step that change from step to step (view, target image, iteration,
@@ -135,27 +134,36 @@ struct TileFinish {
     int tiles;
 };
 // Stable LSD radix sort of (key, value) pairs on key bits [0, bits); the item count is read on the
-// device from *nDev (at most nMax); the initial values are the item indices. Result in *keysOut /
-// *valsOut (one of the two buffers).
+// device from *nDev (at most nMax), or, with nDev null, is nHost (known on the host; at most nMax);
+// the initial values are the item indices. Result in *keysOut / *valsOut (one of the two buffers).
 // Returns the number of passes; rowTotals needs radixDigits() entries. fin (may be null) applies when
 // bits <= 11 (one pass): *keysOut is then not written.
 int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
-                   const TileFinish *fin = nullptr);
+                   const TileFinish *fin = nullptr, int nHost = 0);
 int radixDigits();
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
+// The same scan of per-rank tile counts, fused with the bin pass's capacity check (launchCapacityCheck
+// on the total out[n], done by the scan's last kernel).
+struct ScanCapacity {
+    int capacity;
+    BinCounts *counts;
+    int iteration;
+    const StepDesc *desc;
+};
+void exclusiveScanChecked(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s);
 // Per depth rank: tile count of the Gaussian and the inverse map gid -> rank. With cullRec (the
 // projected records), only the tiles of the rectangle that the contributing ellipse can reach count,
 // and rowTab (cullRowEntries(n) entries) receives the rows' spans for the emission.
 size_t cullRowEntries(size_t n);
 void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
                       int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s);
-// Sets counts->n and checks *total against the intersection capacity (see BinCounts).
+// Checks *total against the intersection capacity (see BinCounts); exclusiveScanChecked does the same
+// inside its last kernel.
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
                          const StepDesc *desc = nullptr);
-void launchSetCount(BinCounts *c, int n, cudaStream_t s);
 // Emission of the intersections in depth-rank order: tile key and Gaussian id per intersection (the
 // same tiles as launchRankCounts counted).
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,

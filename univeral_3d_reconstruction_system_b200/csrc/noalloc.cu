@@ -6,7 +6,7 @@
 // temporaries live in one file-scope device array, so the call makes no cudaMalloc, no cudaFree and
 // no call into an allocating library routine.
 //
-// Scratch (gNoAllocScratch, 11.1 MB per device context that uses this entry point):
+// Scratch (gNoAllocScratch, 11.2 MB per device context that uses this entry point):
 //   [0, 3 * kMaxBlocks) doubles      per-block sums (L1, SSIM, squared error), 3 per loss block
 //   next 4 floats                    total, L1, SSIM, PSNR from the finalize kernel
 //   from a 256-byte boundary         the SSIM partial maps, 9 floats per pixel
@@ -15,8 +15,9 @@
 // of every pixel before the backward kernel reads them, and with lambda = 0 no kernel reads them;
 // the finalize kernel writes the four values).
 //
-// Limits: width * height <= kMaxPixels (640 x 480) and at most kMaxBlocks loss blocks (32 x 16
-// pixels each); larger requests are rejected with U3DG_ERR_CAPACITY before anything is launched.
+// Limits: width * height <= kMaxPixels (640 x 480) and at most 2048 blocks of 32 x 16 pixels (the
+// loss kernels run one CTA per block and channel: kMaxBlocks = 3 x 2048); larger requests are
+// rejected with U3DG_ERR_CAPACITY before anything is launched.
 //
 // Set-up: the first call in each device context, with that device current, resolves the array's
 // address there with cudaGetSymbolAddress (which loads this module into the context) and keeps it
@@ -45,7 +46,7 @@ using namespace u3dg;
 namespace {
 
 constexpr size_t kMaxPixels = 640 * 480;
-constexpr int kMaxBlocks = 2048;
+constexpr int kMaxBlocks = 3 * 2048; // 2048 tiles of 32x16 pixels, one loss block per tile and channel
 constexpr size_t kSumsDoubles = 3 * size_t(kMaxBlocks);
 constexpr size_t kValsOffset = kSumsDoubles;                           // in doubles; 4 floats = 2 doubles
 constexpr size_t kMapsOffset = (kValsOffset + 2 + 31) / 32 * 32;       // 256-byte boundary, in doubles
