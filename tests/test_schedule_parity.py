@@ -10,8 +10,8 @@ Neither side has one "true" final PSNR. With more than one thread the reference 
 thousand steps with densification amplifies such rounding differences: its runs spread over about
 0.15 dB. The GPU trainer is deterministic for a given summation order, and its equally valid orders
 (tile sizes 8, 16 and 32; tile culling on or off, which shifts the order in which a Gaussian's per-tile
-partials are added) spread as much. So the north star's bar, the final evaluatePsnr within 0.1 dB, is
-applied to the means: the mean over those six GPU orders against the mean of the recorded reference
+partials are added) spread as much. So the bar, the final evaluatePsnr within 0.1 dB, is applied to
+the means: the mean over those six GPU orders against the mean of the recorded reference
 runs. Each single GPU run must also stay within 0.3 dB of the reference mean.
 
 Fast (2000 iterations), Balanced (4000, opacity reset at 3000) and High (forIterations(7000), max

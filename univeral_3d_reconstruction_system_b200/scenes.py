@@ -48,7 +48,7 @@ class SceneSpec:
 
 
 PRESETS = {
-    # Fast / Balanced / High.
+    # The Fast / Balanced / High benchmark presets.
     "fast": SceneSpec("fast", 30_000, 32, 320, 240, 300.0, "ring", 5_000, 2000, 80_000),
     "balanced": SceneSpec("balanced", 100_000, 80, 480, 360, 450.0, "two_rings", 15_000, 4000, 150_000,
                           opacity_reset_at=3000),
