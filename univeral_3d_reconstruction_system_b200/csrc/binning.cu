@@ -23,7 +23,7 @@
 // in-block ranks come from warp match-any votes. Every block owns one contiguous chunk of the items
 // and walks it in rounds of kTile items.
 
-#include "kernels.h"
+#include "tile_cull.cuh"
 
 #include <algorithm>
 #include <climits>
@@ -129,9 +129,9 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G,
 // memory; an item's position is its digit's base + the counts of the warps before it (they hold
 // earlier items) + its rank in its warp. After the round the last item of each (warp, digit) advances
 // the digit's base and clears that count, so only the touched counts are reset.
-// kTiles (the single pass of a tile sort, digit = tile): instead of the sorted keys, the scatter
-// writes each entry's Gaussian id (fin.list[pos] = fin.emitGid[emission index]), and block 0 writes
-// the tile offsets, which are the digit bases it starts from.
+// kTiles (the single pass of a tile sort, digit = tile): instead of the sorted keys and values, the
+// scatter writes each entry's (Gaussian id, emission index) pair (fin.entries[pos]), and block 0
+// writes the tile offsets, which are the digit bases it starts from.
 template <int DB, bool kTiles = false>
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
                                                                uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
@@ -204,11 +204,11 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
                     cross += warpCounts[w][d];
                 const int pos = base[d] + cross + local[r];
                 if (kTiles) {
-                    fin.list[pos] = fin.emitGid[val[r]];
+                    fin.entries[pos] = make_int2(fin.emitGid[val[r]], int(val[r]));
                 } else {
                     keysOut[pos] = key[r];
+                    valsOut[pos] = val[r];
                 }
-                valsOut[pos] = val[r];
                 last[r] = local[r] == int(myCounts[d]) - 1;
             }
         }
@@ -246,7 +246,14 @@ __device__ __forceinline__ void checkCapacity(int t, int capacity, BinCounts *c,
 // Exclusive scan, reduce-then-scan over a host-known n.
 constexpr int kScanTile = kThreads * 8;
 
-__global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int n, int *partial)
+// The scan's input element i: in[i], or in[perm[i]] with a permutation (the per-Gaussian tile counts
+// taken in depth-rank order).
+__device__ __forceinline__ int scanInput(const int *in, const uint32_t *perm, int i)
+{
+    return in[perm ? int(perm[i]) : i];
+}
+
+__global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, const uint32_t *perm, int n, int *partial)
 {
     pdlEntry();
     const int base = blockIdx.x * kScanTile;
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(kThreads) scanReduceKernel(const int *in, int 
     for (int r = 0; r < 8; ++r) {
         const int i = base + r * kThreads + threadIdx.x;
         if (i < n)
-            s += in[i];
+            s += scanInput(in, perm, i);
     }
     int total;
     blockExclusiveScan(s, total);
@@ -281,8 +288,8 @@ __global__ void __launch_bounds__(kThreads) scanPartialKernel(int *partial, int 
 }
 
 // cap.counts (may be null): block 0 also runs the bin pass's capacity check on the total.
-__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, int *out, int n, const int *partial, int B,
-                                                                ScanCapacity cap)
+__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, const uint32_t *perm, int *out, int n,
+                                                                const int *partial, int B, ScanCapacity cap)
 {
     pdlEntry();
     const int base = blockIdx.x * kScanTile + threadIdx.x * 8;
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
     int s = 0;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-        v[r] = (base + r < n) ? in[base + r] : 0;
+        v[r] = (base + r < n) ? scanInput(in, perm, base + r) : 0;
         s += v[r];
     }
     int total;
@@ -306,107 +313,6 @@ __global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const int *in, i
         if (cap.counts != nullptr)
             checkCapacity(partial[B], cap.capacity, cap.counts, cap.iteration, cap.desc);
     }
-}
-
-// Tile culling (trainers): a Gaussian is listed only in the tiles of its rectangle that its
-// contributing ellipse {d : A dx^2 + 2 B dx dy + C dy^2 <= t} (power >= powMin) can reach. In one tile
-// row the reachable tiles are contiguous: the ellipse cut by the row's strip of pixel centres spans
-// [xL, xR] with xR(dy) = (-B dy + sqrt(A t - det dy^2)) / A concave in dy, so its maximum over the
-// strip is at the clamped dy of the ellipse's rightmost point (and xL's minimum symmetrically).
-// Rounding-explicit (the count and the emission kernels get the same spans) and conservative like
-// the compositing kernels' block masks: t widened by 4% + 1e-3 and the span by one pixel each side.
-// Dropping entries that reach no pixel of a tile changes no image and no per-entry gradient.
-constexpr int kCullRows = 8; // rows per rank in the emission's row table (32 bytes: two uint4 loads)
-static_assert(kCullRows == 8, "the emission reads a rank's row table as two uint4");
-
-struct CullShape {
-    float mx, my, B, det, at, iA, ymax, dyR; // dyR: dy of the rightmost point, (-B / C) xmax
-    int mode;                                // 0: whole rectangle, 1: no tile, 2: culled rows
-};
-
-__device__ __forceinline__ CullShape cullShape(const SplatRec *rec, int g)
-{
-    const float4 *r = reinterpret_cast<const float4 *>(rec) + size_t(g) * 3;
-    const float4 p = r[0], q = r[1];
-    const float powMin = r[2].w;
-    CullShape c{};
-    const float t = __fadd_rn(__fmul_rn(-2.08f, powMin), 1e-3f);
-    const float det = __fsub_rn(__fmul_rn(q.x, q.z), __fmul_rn(q.y, q.y));
-    // Infinite box extents: ill-conditioned covariance or no alpha floor.
-    if (!(p.z < __int_as_float(0x7f800000)) || !(det > 0.0f) || !(q.x > 0.0f) || !(q.z > 0.0f))
-        return c;
-    if (!(t > 0.0f)) { // alpha below the floor everywhere
-        c.mode = 1;
-        return c;
-    }
-    c.mode = 2;
-    c.mx = p.x;
-    c.my = p.y;
-    c.B = q.y;
-    c.det = det;
-    c.at = __fmul_rn(q.x, t);
-    c.iA = __frcp_rn(q.x);
-    c.ymax = __fsqrt_rn(__fdiv_rn(__fmul_rn(t, q.x), det));
-    const float xmax = __fsqrt_rn(__fdiv_rn(__fmul_rn(t, q.z), det));
-    c.dyR = __fmul_rn(__fdiv_rn(-q.y, q.z), xmax);
-    return c;
-}
-
-// Tile columns [c0, c1) of tile row ty that the ellipse can reach, within rectangle q.
-__device__ __forceinline__ void cullSpan(const CullShape &c, const int4 &q, int ty, int tileSize, int &c0, int &c1)
-{
-    c0 = q.x;
-    c1 = q.z;
-    if (c.mode == 0)
-        return;
-    const float Y0 = __fsub_rn(float(ty * tileSize), c.my), Y1 = __fadd_rn(Y0, float(tileSize - 1));
-    const float lo = fmaxf(Y0, -c.ymax), hi = fminf(Y1, c.ymax);
-    if (c.mode == 1 || lo > hi) {
-        c1 = c0;
-        return;
-    }
-    const float dyR = fminf(fmaxf(c.dyR, lo), hi), dyL = fminf(fmaxf(-c.dyR, lo), hi);
-    const float sR = __fsqrt_rn(fmaxf(__fsub_rn(c.at, __fmul_rn(c.det, __fmul_rn(dyR, dyR))), 0.0f));
-    const float sL = __fsqrt_rn(fmaxf(__fsub_rn(c.at, __fmul_rn(c.det, __fmul_rn(dyL, dyL))), 0.0f));
-    const float xR = __fmul_rn(__fadd_rn(__fmul_rn(-c.B, dyR), sR), c.iA);
-    const float xL = __fmul_rn(__fsub_rn(__fmul_rn(-c.B, dyL), sL), c.iA);
-    const float inv = 1.0f / float(tileSize); // exact: tile sizes are powers of two
-    const float left = floorf(__fmul_rn(__fsub_rn(__fadd_rn(c.mx, xL), 1.0f), inv));
-    const float right = floorf(__fmul_rn(__fadd_rn(__fadd_rn(c.mx, xR), 1.0f), inv)) + 1.0f;
-    c0 = left > float(q.x) ? int(fminf(left, float(q.z))) : q.x;
-    c1 = right < float(q.z) ? int(fmaxf(right, float(q.x))) : q.z;
-    c1 = max(c1, c0);
-}
-
-// With culling, the first kCullRows rows of every rank's rectangle are also recorded in rowTab[rank *
-// kCullRows + i] as (first column << 16) | (tiles through row i), so the emission finds an entry's row
-// without recomputing spans (rows beyond kCullRows, rare, are recomputed there).
-__global__ void rankCountsKernel(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                                 int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab)
-{
-    pdlEntry();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n)
-        return;
-    const int g = int(sortedIds[r]);
-    rankOf[g] = r;
-    int c = 0;
-    if (radius[g] > 0) {
-        const int4 q = rect[g];
-        if (cullRec == nullptr) {
-            c = (q.z - q.x) * (q.w - q.y);
-        } else {
-            const CullShape cs = cullShape(cullRec, g);
-            for (int ty = q.y; ty < q.w; ++ty) {
-                int c0, c1;
-                cullSpan(cs, q, ty, tileSize, c0, c1);
-                c += c1 - c0;
-                if (ty - q.y < kCullRows)
-                    rowTab[size_t(r) * kCullRows + (ty - q.y)] = (uint32_t(c0) << 16) | uint32_t(c);
-            }
-        }
-    }
-    cnt[r] = c;
 }
 
 // Capacity check of a bin pass on its scan total (checkCapacity), when the scan had no kernels to
@@ -464,10 +370,10 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
                     ty = qy + k / wdt;
                     tx = qx + k % wdt;
                 } else {
-                    // The k-th reachable tile in row-major order: the rank's row table, then (rows
+                    // The k-th reachable tile in row-major order: the Gaussian's row table, then (rows
                     // beyond it) the rows' spans.
-                    // One 32-byte row (two vector loads) per rank; entries past its rows are unused.
-                    const uint4 *tab = reinterpret_cast<const uint4 *>(rowTab + size_t(w * 32 + l) * kCullRows);
+                    // One 32-byte row (two vector loads) per Gaussian; entries past its rows are unused.
+                    const uint4 *tab = reinterpret_cast<const uint4 *>(rowTab + size_t(gl) * kCullRows);
                     const uint4 t0 = tab[0], t1 = tab[1];
                     const uint32_t tv[kCullRows] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
                     const int rows = qw - qy;
@@ -511,12 +417,14 @@ __global__ void __launch_bounds__(256) emitKernel(const uint32_t *sortedIds, con
     }
 }
 
-__global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c, int *list)
+__global__ void finalizeKernel(const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c, int2 *entries)
 {
     pdlEntry();
     const int total = c->effTotal;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x)
-        list[s] = emitGid[sortedEmit[s]];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+        const uint32_t e = sortedEmit[s];
+        entries[s] = make_int2(emitGid[e], int(e));
+    }
 }
 
 __global__ void tileOffsetsKernel(const uint32_t *sortedKeys, const BinCounts *c, int tiles, int *tileOffsets)
@@ -587,12 +495,13 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
 
 size_t scanPartialEntries(int n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
 
-static void scanLaunches(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s)
+static void scanLaunches(const int *in, const uint32_t *perm, int *out, int n, int *partial, const ScanCapacity &cap,
+                         cudaStream_t s)
 {
     const int B = (n + kScanTile - 1) / kScanTile;
-    { launchPdl(scanReduceKernel, B, kThreads, 0, s, in, n, partial); countLaunch(); }
+    { launchPdl(scanReduceKernel, B, kThreads, 0, s, in, perm, n, partial); countLaunch(); }
     { launchPdl(scanPartialKernel, 1, kThreads, 0, s, partial, B); countLaunch(); }
-    { launchPdl(scanDownsweepKernel, B, kThreads, 0, s, in, out, n, partial, B, cap); countLaunch(); }
+    { launchPdl(scanDownsweepKernel, B, kThreads, 0, s, in, perm, out, n, partial, B, cap); countLaunch(); }
 }
 
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
@@ -601,27 +510,22 @@ void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s)
         cudaMemsetAsync(out, 0, sizeof(int), s);
         return;
     }
-    scanLaunches(in, out, n, partial, ScanCapacity{0, nullptr, 0, nullptr}, s);
+    scanLaunches(in, nullptr, out, n, partial, ScanCapacity{0, nullptr, 0, nullptr}, s);
 }
 
-void exclusiveScanChecked(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s)
+void exclusiveScanChecked(const int *in, const uint32_t *perm, int *out, int n, int *partial, const ScanCapacity &cap,
+                          cudaStream_t s)
 {
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(int), s);
         launchCapacityCheck(out, cap.capacity, cap.counts, cap.iteration, s, cap.desc);
         return;
     }
-    scanLaunches(in, out, n, partial, cap, s);
+    scanLaunches(in, perm, out, n, partial, cap, s);
 }
 
 size_t cullRowEntries(size_t n) { return n * kCullRows; }
 
-void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                      int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s)
-{
-    if (n > 0)
-        { launchPdl(rankCountsKernel, grid(n, 256), 256, 0, s, sortedIds, rect, radius, cullRec, tileSize, n, cnt, rankOf, rowTab); countLaunch(); }
-}
 
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
                          const StepDesc *desc)
@@ -638,10 +542,10 @@ void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, in
 }
 
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s)
+                        int capacity, int tiles, int2 *entries, int *tileOffsets, cudaStream_t s)
 {
     if (capacity > 0)
-        { launchPdl(finalizeKernel, std::min(grid(capacity, 256), 148 * 16), 256, 0, s, sortedEmit, emitGid, c, list); countLaunch(); }
+        { launchPdl(finalizeKernel, std::min(grid(capacity, 256), 148 * 16), 256, 0, s, sortedEmit, emitGid, c, entries); countLaunch(); }
     { launchPdl(tileOffsetsKernel, grid(tiles + 1, 256), 256, 0, s, sortedKeys, c, tiles, tileOffsets); countLaunch(); }
 }
 

@@ -641,7 +641,9 @@ int u3dg_rasterizer_tiles(u3dg_rasterizer *r, int *tiles_x, int *tiles_y, int *o
             U3DG_CUDA(cudaMemcpyAsync(offsets, R.ws.tileOffsets.p, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
         const size_t L = std::min(list_capacity, size_t(R.ws.total()));
         if (list && L)
-            U3DG_CUDA(cudaMemcpyAsync(list, R.ws.list.p, L * sizeof(int), cudaMemcpyDeviceToHost, s));
+            // The Gaussian ids: the first int of each (id, emission index) entry.
+            U3DG_CUDA(cudaMemcpy2DAsync(list, sizeof(int), R.ws.entries.p, sizeof(int2), sizeof(int), L,
+                                        cudaMemcpyDeviceToHost, s));
         R.stream.sync();
     });
 }
@@ -701,12 +703,12 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
         ws.sortVals1.reserve(nn);
         ws.rect.reserve(nn);
         ws.radius.reserve(nn);
-        ws.rankOf.reserve(nn);
         ws.cnt.reserve(nn);
         ws.offs.reserve(nn + 1);
         ws.scanPartial.reserve(scanPartialEntries(int(nn)) + 1);
         std::vector<uint32_t> keys(n);
         std::vector<int4> rc(n);
+        std::vector<int> cnt(n); // tiles per Gaussian: its whole rectangle (no culling at this boundary)
         for (size_t i = 0; i < n; ++i) {
             uint32_t b;
             std::memcpy(&b, &depth[i], 4);
@@ -715,6 +717,7 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
             if (radius[i] > 0 && (rc[i].x < 0 || rc[i].y < 0 || rc[i].z > tiles_x || rc[i].w > tiles_y ||
                                   rc[i].x >= rc[i].z || rc[i].y >= rc[i].w))
                 throw StatusError(U3DG_ERR_INVALID_ARG, "rect of a visible Gaussian is outside the tile grid");
+            cnt[i] = radius[i] > 0 ? (rc[i].z - rc[i].x) * (rc[i].w - rc[i].y) : 0;
         }
         ws.reserveIntersections(std::max<size_t>(size_t(1) << 16, 4 * nn));
         for (int attempt = 0;; ++attempt) {
@@ -723,6 +726,7 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
                 U3DG_CUDA(cudaMemcpyAsync(ws.depthKey.p, keys.data(), n * 4, cudaMemcpyHostToDevice, st.s));
                 U3DG_CUDA(cudaMemcpyAsync(ws.rect.p, rc.data(), n * sizeof(int4), cudaMemcpyHostToDevice, st.s));
                 U3DG_CUDA(cudaMemcpyAsync(ws.radius.p, radius, n * sizeof(int), cudaMemcpyHostToDevice, st.s));
+                U3DG_CUDA(cudaMemcpyAsync(ws.cnt.p, cnt.data(), n * sizeof(int), cudaMemcpyHostToDevice, st.s));
             }
             ws.clearCounts(st.s);
             ws.bin(st.s, 0);
@@ -739,7 +743,8 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
         U3DG_CUDA(cudaMemcpyAsync(offsets, ws.tileOffsets.p, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost, st.s));
         const size_t L = std::min(list_capacity, size_t(ws.total()));
         if (list && L)
-            U3DG_CUDA(cudaMemcpyAsync(list, ws.list.p, L * sizeof(int), cudaMemcpyDeviceToHost, st.s));
+            U3DG_CUDA(cudaMemcpy2DAsync(list, sizeof(int), ws.entries.p, sizeof(int2), sizeof(int), L,
+                                        cudaMemcpyDeviceToHost, st.s));
         if (list_length)
             *list_length = size_t(ws.total());
         st.sync();

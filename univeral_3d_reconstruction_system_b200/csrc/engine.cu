@@ -134,7 +134,7 @@ void RasterWorkspace::eachIntersectionBuffer(size_t capacity, F &&f)
     f(iVals0, capacity);
     f(iVals1, capacity);
     f(emitGid, capacity);
-    f(list, capacity);
+    f(entries, capacity);
     f(partial, capacity * kG2d * size_t(partialSlots));
 }
 
@@ -173,7 +173,7 @@ void RasterWorkspace::project(const Params &P, int count, const u3dg_camera &c, 
         partialSlots = per * per;
         partial.reserve(size_t(icap) * kG2d * size_t(partialSlots), true);
     }
-    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p};
+    ProjOut out{rec.p, depthKey.p, depth.p, rect.p, radius.p, flags.p, cov2d.p, cnt.p, rowTab.p, culled() ? 1 : 0};
     launchProject(P, n, cam, st, tilesX, tilesY, shRest, shDegree, out, stream, desc);
 }
 
@@ -188,7 +188,6 @@ void RasterWorkspace::eachGaussianBuffer(size_t nn, F &&f)
     f(depth, nn);
     f(rect, nn);
     f(radius, nn);
-    f(rankOf, nn);
     f(rowTab, cullRowEntries(nn));
     f(cnt, nn);
     f(offs, nn + 1);
@@ -232,23 +231,23 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, nullptr, std::max(n, 1), 32, hist.p, rowTotals.p,
                    &keysOut, &valsOut, stream, nullptr, n);
     sortedIds = valsOut;
-    // The emission's row table packs cumulative counts of 8 rows in 16 bits: rows of at most 8191 tiles.
-    const SplatRec *cullRec = (cullTiles && tilesX < 8192) ? rec.p : nullptr;
-    launchRankCounts(sortedIds, rect.p, radius.p, cullRec, st.tile_size, n, cnt.p, rankOf.p, rowTab.p, stream);
-    exclusiveScanChecked(cnt.p, offs.p, n, scanPartial.p, ScanCapacity{icap, counts.p, iteration, desc}, stream);
+    // The projection counted each Gaussian's tiles (and, culling, its row table); the scan takes the
+    // counts in depth-rank order.
+    const SplatRec *cullRec = culled() ? rec.p : nullptr;
+    exclusiveScanChecked(cnt.p, sortedIds, offs.p, n, scanPartial.p, ScanCapacity{icap, counts.p, iteration, desc},
+                         stream);
     launchEmit(sortedIds, offs.p, rect.p, n, counts.p, icap, tilesX, cullRec, st.tile_size, rowTab.p, iKeys0.p,
                emitGid.p, stream);
     int bits = 0;
     while ((1 << bits) < tiles)
         ++bits;
     bits = std::max(bits, 1);
-    // Up to 2048 tiles: one pass whose scatter also writes the lists' Gaussian ids and the tile offsets.
-    const TileFinish fin{emitGid.p, list.p, tileOffsets.p, tiles};
+    // Up to 2048 tiles: one pass whose scatter also writes the lists' entries and the tile offsets.
+    const TileFinish fin{emitGid.p, entries.p, tileOffsets.p, tiles};
     const int tilePasses = radixSortPairs(iKeys0.p, iKeys1.p, iVals0.p, iVals1.p, &counts.p->effTotal, icap, bits,
                                           hist.p, rowTotals.p, &keysOut, &valsOut, stream, &fin);
-    listEmit = valsOut;
     if (tilePasses != 1)
-        launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, list.p, tileOffsets.p, stream);
+        launchFinalizeBins(keysOut, valsOut, emitGid.p, counts.p, icap, tiles, entries.p, tileOffsets.p, stream);
 }
 
 void RasterWorkspace::forwardChecked(const Params &P, int count, const u3dg_camera &c, const u3dg_raster_settings &s,
@@ -270,8 +269,7 @@ RasterArgs RasterWorkspace::rasterArgs() const
 {
     RasterArgs a;
     a.tileOffsets = tileOffsets.p;
-    a.list = list.p;
-    a.listEmit = listEmit;
+    a.entries = entries.p;
     a.rec = rec.p;
     a.width = cam.width;
     a.height = cam.height;
@@ -326,7 +324,6 @@ ChainArgs RasterWorkspace::chainArgs(const Params &P) const
     a.radius = radius.p;
     a.rec = rec.p;
     a.flags = flags.p;
-    a.rankOf = rankOf.p;
     a.offs = offs.p;
     a.sortedIds = sortedIds;
     a.partial = partial.p;

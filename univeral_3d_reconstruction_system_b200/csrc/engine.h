@@ -197,15 +197,15 @@ struct RasterWorkspace {
     DevBuf<uint32_t> depthKey, sortKeys, sortVals0, sortVals1;
     DevBuf<float> depth;
     DevBuf<int4> rect;
-    DevBuf<int> radius, rankOf, cnt, offs, scanPartial, hist, rowTotals;
-    DevBuf<uint32_t> rowTab; // tile culling: per rank, the first rows' spans (emission lookup)
+    DevBuf<int> radius, cnt, offs, scanPartial, hist, rowTotals; // cnt: tiles per Gaussian (projection)
+    DevBuf<uint32_t> rowTab; // tile culling: per Gaussian, the first rows' spans (emission lookup)
     DevBuf<uint8_t> flags;
     DevBuf<float4> cov2d;
     DevBuf<float> g2d; // per Gaussian: summed 2D gradients (chain-rule input)
     // per intersection (capacity icap)
     DevBuf<uint32_t> iKeys0, iKeys1, iVals0, iVals1;
-    DevBuf<int> emitGid, list;
-    uint32_t *listEmit = nullptr; // emission index per tile-sorted entry (one of iVals0 / iVals1)
+    DevBuf<int> emitGid;
+    DevBuf<int2> entries; // per tile-sorted entry: Gaussian id, emission index
     DevBuf<float> partial;             // partialSlots arrays of icap * 9 floats
     int icap = 0;
     int partialSlots = 1;              // slot arrays the backward needs: (tile size / 16)^2 above 16
@@ -225,6 +225,8 @@ struct RasterWorkspace {
     // Tile culling: list a Gaussian only in the tiles of its rectangle that its contributing ellipse
     // can reach (trainers; the rasterizer unit boundary keeps the reference's lists).
     bool cullTiles = false;
+    // Culling applies while tile rows fit the row table's 16-bit cumulative counts (< 8192 tiles).
+    bool culled() const { return cullTiles && tilesX < 8192; }
     u3dg_camera cam{};
     u3dg_raster_settings st{};
     uint32_t *sortedIds = nullptr;

@@ -6,7 +6,7 @@
 // except where glibc's expf differs from the correctly rounded exp used here (expCR).
 // All of these kernels stream over Gaussians and are HBM-bound.
 
-#include "kernels.h"
+#include "tile_cull.cuh"
 
 #include <cfloat>
 #include <climits>
@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
         out.rect[i] = make_int4(0, 0, 0, 0);
         out.depthKey[i] = 0xFFFFFFFFu;
         out.flags[i] = 0;
+        out.tileCount[i] = 0;
         return;
     }
     const float invDet = 1.0f / det;
@@ -164,6 +165,18 @@ __global__ void __launch_bounds__(256) projectKernel(Params P, int n, u3dg_camer
     out.radius[i] = radius;
     out.depth[i] = p.pc[2];
     out.depthKey[i] = __float_as_uint(p.pc[2]);
+    // The tiles it is listed in (Rasterizer.cpp:206-261 lists the whole rectangle; the trainers only the
+    // tiles its contributing ellipse reaches), counted here where the record is in registers; the
+    // binning scans the counts in depth order.
+    int tiles = 0;
+    if (radius > 0) {
+        const bool cull = out.cullTiles != 0;
+        const CullShape cs = cull ? cullShapeOf(make_float4(r.mx, r.my, r.ex, r.ey), make_float4(r.A, r.B, r.C, r.alpha),
+                                                r.powMin)
+                                  : CullShape{};
+        tiles = listedTiles(cs, cull, rect, ts, cull ? out.rowTab + size_t(i) * kCullRows : nullptr);
+    }
+    out.tileCount[i] = tiles;
 }
 
 // One Adam element update (adamArray, Adam.cpp:13-28), same order as the reference.

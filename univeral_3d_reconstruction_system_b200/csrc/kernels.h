@@ -71,6 +71,9 @@ struct ProjOut {
     int *radius;        // 0 = not visible
     uint8_t *flags;     // bit0/1: J clamped in x/y; bit2..4: colour clamped
     float4 *cov2d;      // 2D covariance a, b, c (including eps2d), for inspection
+    int *tileCount;     // tiles the Gaussian is listed in (0 when not visible)
+    uint32_t *rowTab;   // tile culling: the first rows' spans (tile_cull.cuh, listedTiles); may be null
+    int cullTiles;      // 1: list only the tiles the contributing ellipse reaches (then rowTab is set)
 };
 
 // Arguments of the chain-rule kernel (backward pass 2), optionally fused with Adam.
@@ -82,7 +85,6 @@ struct ChainArgs {
     const int *radius;
     const SplatRec *rec;
     const uint8_t *flags;
-    const int *rankOf;    // depth rank of every Gaussian
     const int *offs;      // per rank: first intersection in emission order (n + 1 entries)
     const uint32_t *sortedIds; // Gaussian id per depth rank
     const float *partial; // per intersection, in emission order: 9 summed 2D gradients (subSlots arrays)
@@ -124,12 +126,14 @@ void launchOpacityReset(float *opac, float *mOpac, float *vOpac, int n, float ca
 // Blocks of a radix pass sized for at most nMax items, and the histogram entries it needs.
 int radixBlocks(int nMax);
 size_t radixHistEntries(int nMax);
-// Outputs of a tile sort done in one pass (keys of at most 11 bits, digit = tile): the scatter writes
-// the Gaussian id of every sorted entry (list[pos] = emitGid[emission index]) instead of the sorted
-// keys, and the tile offsets (tiles + 1 entries; the last is the item count).
+// Outputs of a tile sort done in one pass (keys of at most 11 bits, digit = tile): instead of the
+// sorted keys and values, the scatter writes every sorted entry as one 8-byte pair (entries[pos] =
+// (Gaussian id = emitGid[emission index], emission index)), and the tile offsets (tiles + 1 entries;
+// the last is the item count). One scattered 8-byte store per entry instead of two 4-byte ones: the
+// scatter's cost is its scattered stores.
 struct TileFinish {
     const int *emitGid;
-    int *list;
+    int2 *entries;
     int *tileOffsets;
     int tiles;
 };
@@ -137,7 +141,7 @@ struct TileFinish {
 // device from *nDev (at most nMax), or, with nDev null, is nHost (known on the host; at most nMax);
 // the initial values are the item indices. Result in *keysOut / *valsOut (one of the two buffers).
 // Returns the number of passes; rowTotals needs radixDigits() entries. fin (may be null) applies when
-// bits <= 11 (one pass): *keysOut is then not written.
+// bits <= 11 (one pass): the sorted keys and values are then not written (fin->entries instead).
 int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *valsB, const int *nDev, int nMax,
                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
                    const TileFinish *fin = nullptr, int nHost = 0);
@@ -145,21 +149,18 @@ int radixDigits();
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
-// The same scan of per-rank tile counts, fused with the bin pass's capacity check (launchCapacityCheck
-// on the total out[n], done by the scan's last kernel).
+// The scan of in[perm[i]] (the per-Gaussian tile counts in depth-rank order), fused with the bin pass's
+// capacity check (launchCapacityCheck on the total out[n], done by the scan's last kernel).
 struct ScanCapacity {
     int capacity;
     BinCounts *counts;
     int iteration;
     const StepDesc *desc;
 };
-void exclusiveScanChecked(const int *in, int *out, int n, int *partial, const ScanCapacity &cap, cudaStream_t s);
-// Per depth rank: tile count of the Gaussian and the inverse map gid -> rank. With cullRec (the
-// projected records), only the tiles of the rectangle that the contributing ellipse can reach count,
-// and rowTab (cullRowEntries(n) entries) receives the rows' spans for the emission.
+void exclusiveScanChecked(const int *in, const uint32_t *perm, int *out, int n, int *partial, const ScanCapacity &cap,
+                          cudaStream_t s);
+// Entries of the per-Gaussian row table of tile culling (ProjOut::rowTab) for n Gaussians.
 size_t cullRowEntries(size_t n);
-void launchRankCounts(const uint32_t *sortedIds, const int4 *rect, const int *radius, const SplatRec *cullRec,
-                      int tileSize, int n, int *cnt, int *rankOf, uint32_t *rowTab, cudaStream_t s);
 // Checks *total against the intersection capacity (see BinCounts); exclusiveScanChecked does the same
 // inside its last kernel.
 void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int iteration, cudaStream_t s,
@@ -169,16 +170,16 @@ void launchCapacityCheck(const int *total, int capacity, BinCounts *c, int itera
 void launchEmit(const uint32_t *sortedIds, const int *offs, const int4 *rect, int n, const BinCounts *c, int capacity,
                 int tilesX, const SplatRec *cullRec, int tileSize, const uint32_t *rowTab, uint32_t *keys, int *emitGid,
                 cudaStream_t s);
-// After a tile sort of several passes (more than 2048 tiles): Gaussian id per sorted entry and the tile
-// offsets (a binary search in the sorted keys). A one-pass tile sort writes both itself (TileFinish).
+// After a tile sort of several passes (more than 2048 tiles): the (Gaussian id, emission index) pair of
+// every sorted entry and the tile offsets (a binary search in the sorted keys). A one-pass tile sort
+// writes both itself (TileFinish).
 void launchFinalizeBins(const uint32_t *sortedKeys, const uint32_t *sortedEmit, const int *emitGid, const BinCounts *c,
-                        int capacity, int tiles, int *list, int *tileOffsets, cudaStream_t s);
+                        int capacity, int tiles, int2 *entries, int *tileOffsets, cudaStream_t s);
 
 // raster.cu
 struct RasterArgs {
     const int *tileOffsets;
-    const int *list;          // Gaussian id per tile-sorted entry
-    const uint32_t *listEmit; // emission index per tile-sorted entry (where backward stores partials)
+    const int2 *entries; // per tile-sorted entry: Gaussian id, emission index (where backward stores partials)
     const SplatRec *rec;
     int width, height, tileSize, tilesX;
     float bg[3];

@@ -49,7 +49,7 @@ __device__ __forceinline__ void forwardBlock(const RasterArgs &a, int bx, int by
 #pragma unroll
         for (int r = 0; r < BD; ++r) {
             const int slot = r * NT + tid;
-            stage<PB, BD>(rec, a.list, b0 + slot, b0 + slot < end, slot, sP, sQ, sR, mask, bx, by);
+            stage<PB, BD>(rec, a.entries, b0 + slot, b0 + slot < end, slot, sP, sQ, sR, mask, bx, by);
         }
         __syncthreads();
         for (int k = 0; k < NG && !(done0 && done1); ++k) {

@@ -151,7 +151,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
     // accumulators start at zero); their partials are still written, as the chain-rule kernel sums
     // every intersection of a Gaussian.
     for (int j = jmax + tid; j < end - start; j += NT) {
-            float *dst = partial + size_t(a.listEmit[start + j]) * kG2d;
+            float *dst = partial + size_t(a.entries[start + j].y) * kG2d;
 #pragma unroll
             for (int k = 0; k < kG2d; ++k)
                 dst[k] = 0.0f;
@@ -163,7 +163,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
 #pragma unroll
         for (int r = 0; r < BD; ++r) {
             const int slot = r * NT + tid;
-            stage<PB, BD>(rec, a.list, start + bStart + slot, slot < cnt, slot, sP, sQ, sR, mask, bx, by);
+            stage<PB, BD>(rec, a.entries, start + bStart + slot, slot < cnt, slot, sP, sQ, sR, mask, bx, by);
         }
         {
             float4 *z = reinterpret_cast<float4 *>(sWarp);
@@ -280,7 +280,7 @@ __device__ __forceinline__ void backwardBlock(const RasterArgs &a, int bx, int b
                 for (int q = 0; q < kG2d; ++q)
                     sum[q] += sWarp[(size_t(w) * NB + e) * kG2d + q];
             finishEntry(sQ[e], sum);
-            float *dst = partial + size_t(a.listEmit[start + bStart + e]) * kG2d;
+            float *dst = partial + size_t(a.entries[start + bStart + e].y) * kG2d;
 #pragma unroll
             for (int q = 0; q < kG2d; ++q)
                 dst[q] = sum[q];

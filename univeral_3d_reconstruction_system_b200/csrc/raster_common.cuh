@@ -109,7 +109,7 @@ __device__ __forceinline__ int nextBlock(const RasterArgs &a, int *counter, int 
 
 // Stages batch entry `slot` (if valid) and the masks: mask[w][g] bit b <=> entry 32g + b meets warp w.
 template <int PB, int BD>
-__device__ __forceinline__ void stage(const float4 *rec, const int *list, int idx, bool valid, int slot, float4 *sP,
+__device__ __forceinline__ void stage(const float4 *rec, const int2 *entries, int idx, bool valid, int slot, float4 *sP,
                                       float4 *sQ, float4 *sR, uint32_t (*mask)[RasterShape<PB, BD>::NG], int bx,
                                       int by)
 {
@@ -117,7 +117,7 @@ __device__ __forceinline__ void stage(const float4 *rec, const int *list, int id
     float4 p = make_float4(0.0f, 0.0f, -1.0f, -1.0f), q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float powMin = 0.0f, iA = 0.0f, iC = 0.0f;
     if (valid) {
-        const float4 *r = rec + size_t(list[idx]) * 3;
+        const float4 *r = rec + size_t(entries[idx].x) * 3;
         p = r[0];
         q = r[1];
         const float4 c = r[2];
