@@ -87,8 +87,9 @@ __device__ __forceinline__ void chunkOf(int n, int G, int b, int &begin, int &en
 }
 
 template <int DB>
-__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const int *nPtr, int nHost, int shift,
-                                                            int *hist, int G)
+// keys, or with pairs set the (key, value) pairs' keys.
+__global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys, const uint2 *pairs, const int *nPtr,
+                                                            int nHost, int shift, int *hist, int G)
 {
     pdlEntry();
     constexpr int R = 1 << DB;
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) radixHistKernel(const uint32_t *keys
     int begin, end;
     chunkOf(nPtr ? *nPtr : nHost, G, blockIdx.x, begin, end);
     for (int i = begin + threadIdx.x; i < end; i += kThreads)
-        atomicAdd(&counts[(keys[i] >> shift) & uint32_t(R - 1)], 1);
+        atomicAdd(&counts[((pairs ? pairs[i].x : keys[i]) >> shift) & uint32_t(R - 1)], 1);
     __syncthreads();
     for (int d = threadIdx.x; d < R; d += kThreads)
         hist[size_t(d) * G + blockIdx.x] = counts[d];
@@ -132,11 +133,19 @@ __global__ void __launch_bounds__(kThreads) radixRowScanKernel(int *hist, int G,
 // kTiles (the single pass of a tile sort, digit = tile): instead of the sorted keys and values, the
 // scatter writes each entry's (Gaussian id, emission index) pair (fin.entries[pos]), and block 0
 // writes the tile offsets, which are the digit bases it starts from.
+// Where a pass of the depth sort keeps its items: (key, value) pairs in and out, so each item is one
+// load and one scattered 8-byte store; the last pass writes the values only (the keys are done).
+struct PairIO {
+    const uint2 *in;    // when set: the items (keysIn / valsIn unused)
+    uint2 *out;         // when set: write (key, value) pairs
+    uint32_t *valsOnly; // when set: write the values only
+};
+
 template <int DB, bool kTiles = false>
 __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *keysIn, const uint32_t *valsIn,
                                                                uint32_t *keysOut, uint32_t *valsOut, const int *nPtr,
                                                                int nHost, int shift, const int *hist, const int *rowTotals,
-                                                               int G, TileFinish fin)
+                                                               int G, TileFinish fin, PairIO io)
 {
     pdlEntry();
     const int n = nPtr ? *nPtr : nHost;
@@ -176,8 +185,14 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
         for (int r = 0; r < kItemsPerThread; ++r) {
             const int i = first + r * 32 + lane;
             const bool valid = i < end;
-            key[r] = valid ? keysIn[i] : 0u;
-            val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
+            if (io.in) {
+                const uint2 kv = valid ? io.in[i] : make_uint2(0u, 0u);
+                key[r] = kv.x;
+                val[r] = kv.y;
+            } else {
+                key[r] = valid ? keysIn[i] : 0u;
+                val[r] = valid ? (valsIn ? valsIn[i] : uint32_t(i)) : 0u;
+            }
             const int d = valid ? int((key[r] >> shift) & uint32_t(R - 1)) : R;
             digit[r] = d;
             local[r] = 0;
@@ -205,6 +220,10 @@ __global__ void __launch_bounds__(kThreads) radixScatterKernel(const uint32_t *k
                 const int pos = base[d] + cross + local[r];
                 if (kTiles) {
                     fin.entries[pos] = make_int2(fin.emitGid[val[r]], int(val[r]));
+                } else if (io.out) {
+                    io.out[pos] = make_uint2(key[r], val[r]);
+                } else if (io.valsOnly) {
+                    io.valsOnly[pos] = val[r];
                 } else {
                     keysOut[pos] = key[r];
                     valsOut[pos] = val[r];
@@ -471,16 +490,16 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     int passes = 0;
     for (int shift = 0; shift < bits; shift += db, ++passes) {
         if (wide) {
-            { launchPdl(radixHistKernel<kWideBits>, G, kThreads, 0, s, kin, nDev, nHost, shift, hist, G); countLaunch(); }
+            { launchPdl(radixHistKernel<kWideBits>, G, kThreads, 0, s, kin, nullptr, nDev, nHost, shift, hist, G); countLaunch(); }
             { launchPdl(radixRowScanKernel, 1 << kWideBits, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
             if (fin != nullptr)
-                { launchPdl(radixScatterKernel<kWideBits, true>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, *fin); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits, true>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, *fin, PairIO{}); countLaunch(); }
             else
-                { launchPdl(radixScatterKernel<kWideBits>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+                { launchPdl(radixScatterKernel<kWideBits>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}, PairIO{}); countLaunch(); }
         } else {
-            { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, kin, nDev, nHost, shift, hist, G); countLaunch(); }
+            { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, kin, nullptr, nDev, nHost, shift, hist, G); countLaunch(); }
             { launchPdl(radixRowScanKernel, 1 << 8, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
-            { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}); countLaunch(); }
+            { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, kin, vin, kout, vout, nDev, nHost, shift, hist, rowTotals, G, TileFinish{}, PairIO{}); countLaunch(); }
         }
         uint32_t *nk = kin;
         kin = kout;
@@ -491,6 +510,22 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
     *keysOut = kin;
     *valsOut = const_cast<uint32_t *>(vin);
     return passes;
+}
+
+void radixSortDepth(const uint32_t *keys, uint2 *pairsA, uint2 *pairsB, uint32_t *sortedIds, int n, int *hist,
+                    int *rowTotals, cudaStream_t s)
+{
+    const int G = radixBlocks(std::max(n, 1));
+    const uint2 *pin = nullptr;
+    uint2 *bufs[2] = {pairsA, pairsB};
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        const PairIO io{pin, pass < 3 ? bufs[pass & 1] : nullptr, pass < 3 ? nullptr : sortedIds};
+        { launchPdl(radixHistKernel<8>, G, kThreads, 0, s, keys, pin, nullptr, n, shift, hist, G); countLaunch(); }
+        { launchPdl(radixRowScanKernel, 1 << 8, kThreads, 0, s, hist, G, rowTotals); countLaunch(); }
+        { launchPdl(radixScatterKernel<8>, G, kThreads, 0, s, keys, nullptr, nullptr, nullptr, nullptr, n, shift, hist, rowTotals, G, TileFinish{}, io); countLaunch(); }
+        pin = io.out;
+    }
 }
 
 size_t scanPartialEntries(int n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }

@@ -698,9 +698,9 @@ int u3dg_bin_tiles(const float *depth, const int *radius, const int *rect, size_
         ws.tilesY = tiles_y;
         const size_t nn = std::max<size_t>(n, 1);
         ws.depthKey.reserve(nn);
-        ws.sortKeys.reserve(nn);
-        ws.sortVals0.reserve(nn);
-        ws.sortVals1.reserve(nn);
+        ws.depthPairs[0].reserve(nn);
+        ws.depthPairs[1].reserve(nn);
+        ws.depthOrder.reserve(nn);
         ws.rect.reserve(nn);
         ws.radius.reserve(nn);
         ws.cnt.reserve(nn);

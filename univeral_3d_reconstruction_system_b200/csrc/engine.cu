@@ -182,9 +182,9 @@ void RasterWorkspace::eachGaussianBuffer(size_t nn, F &&f)
 {
     f(rec, nn);
     f(depthKey, nn);
-    f(sortKeys, nn);
-    f(sortVals0, nn);
-    f(sortVals1, nn);
+    f(depthPairs[0], nn);
+    f(depthPairs[1], nn);
+    f(depthOrder, nn);
     f(depth, nn);
     f(rect, nn);
     f(radius, nn);
@@ -228,9 +228,8 @@ void RasterWorkspace::bin(cudaStream_t stream, int iteration, const StepDesc *de
     rowTotals.reserve(size_t(radixDigits()));
     tileOffsets.reserve(size_t(tiles) + 1);
     uint32_t *keysOut = nullptr, *valsOut = nullptr;
-    radixSortPairs(depthKey.p, sortKeys.p, sortVals0.p, sortVals1.p, nullptr, std::max(n, 1), 32, hist.p, rowTotals.p,
-                   &keysOut, &valsOut, stream, nullptr, n);
-    sortedIds = valsOut;
+    radixSortDepth(depthKey.p, depthPairs[0].p, depthPairs[1].p, depthOrder.p, n, hist.p, rowTotals.p, stream);
+    sortedIds = depthOrder.p;
     // The projection counted each Gaussian's tiles (and, culling, its row table); the scan takes the
     // counts in depth-rank order.
     const SplatRec *cullRec = culled() ? rec.p : nullptr;

@@ -194,7 +194,8 @@ void checkCamera(const u3dg_camera &cam);
 struct RasterWorkspace {
     // per Gaussian
     DevBuf<SplatRec> rec;
-    DevBuf<uint32_t> depthKey, sortKeys, sortVals0, sortVals1;
+    DevBuf<uint32_t> depthKey, depthOrder; // depth sort key per Gaussian; Gaussian ids in depth order
+    DevBuf<uint2> depthPairs[2];           // the depth sort's (key, id) pairs between passes
     DevBuf<float> depth;
     DevBuf<int4> rect;
     DevBuf<int> radius, cnt, offs, scanPartial, hist, rowTotals; // cnt: tiles per Gaussian (projection)

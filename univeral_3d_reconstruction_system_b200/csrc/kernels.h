@@ -146,6 +146,11 @@ int radixSortPairs(uint32_t *keysA, uint32_t *keysB, uint32_t *valsA, uint32_t *
                    int bits, int *hist, int *rowTotals, uint32_t **keysOut, uint32_t **valsOut, cudaStream_t s,
                    const TileFinish *fin = nullptr, int nHost = 0);
 int radixDigits();
+// The depth sort: stable sort of the n 32-bit keys (four 8-bit passes; ties keep index order), items
+// kept as (key, index) pairs between passes (pairsA / pairsB: n each); sortedIds receives the
+// indices in key order.
+void radixSortDepth(const uint32_t *keys, uint2 *pairsA, uint2 *pairsB, uint32_t *sortedIds, int n, int *hist,
+                    int *rowTotals, cudaStream_t s);
 // Exclusive prefix sum of n ints: out[0..n], out[n] = total. partial needs scanPartialEntries(n).
 size_t scanPartialEntries(int n);
 void exclusiveScan(const int *in, int *out, int n, int *partial, cudaStream_t s);
