@@ -398,6 +398,11 @@ int u3dg_trainer_suggest_crop_box(u3dg_trainer *trainer, float low_fraction, flo
 int u3dg_init_gaussians_from_points(const float *xyz, const float *rgb, size_t n, u3dg_model *out);
 /* writeSplatPly (engine/include/u3d/splat/SplatPly.h:12, engine/src/splat/SplatPly.cpp:261-282). */
 int u3dg_write_splat_ply(const char *path, const u3dg_model *model);
+/* No reference counterpart (the reference trainer keeps SH degree 0): writeSplatPly plus the higher-order
+ * SH coefficients as the common 3DGS properties f_rest_0 .. f_rest_{3K-1} after f_dc_2, channel-major
+ * (f_rest_{c*K + k} = sh_rest[(i*K + k)*3 + c], K = (degree+1)^2 - 1, the layout u3dg_render_sh
+ * takes); degree 1..3. u3dg_read_splat_ply and the reference's reader ignore the extra properties. */
+int u3dg_write_splat_ply_sh(const char *path, const u3dg_model *model, const float *sh_rest, int degree);
 /* readSplatPly (SplatPly.h:17-18, SplatPly.cpp:284-342). Call with out == NULL to get *count first.
  * is_splat (may be NULL) reports whether the file held Gaussians or a plain point cloud. */
 int u3dg_read_splat_ply(const char *path, u3dg_model *out, size_t capacity, size_t *count, int *is_splat);

@@ -193,3 +193,33 @@ def test_ascii_numbers(reference, tmp_path):
     path.write_bytes(text)
     ours, splat = assert_same(reference, path)
     assert not splat and ours.size() == 4
+
+
+@pytest.mark.parametrize("degree", [1, 3])
+def test_sh_coefficients_written_as_f_rest(reference, tmp_path, degree):
+    """writeSplatPly with higher-order SH (u3dg_write_splat_ply_sh): the common 3DGS properties
+    f_rest_0 .. f_rest_{3K-1} after f_dc_2, channel-major, and both readers still read the same
+    Gaussians (they ignore the extra properties, SplatPly.cpp:286-288)."""
+    rng = np.random.default_rng(21)
+    n, K = 70_000, (degree + 1) ** 2 - 1  # more than one write block
+    m = GaussianModel(*(rng.normal(size=s).astype(np.float32) for s in ((n, 3), (n, 3), (n, 4), (n,), (n, 3))))
+    sh = rng.normal(size=(n, K, 3)).astype(np.float32)
+    path = tmp_path / "sh.ply"
+    assert api.writeSplatPlySh(str(path), m, sh, degree)
+    data = path.read_bytes()
+    end = data.index(b"end_header\n") + len(b"end_header\n")
+    props = [l.split()[-1] for l in data[:end].decode().splitlines() if l.startswith("property")]
+    rest = [f"f_rest_{i}" for i in range(3 * K)]
+    assert props == ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2", *rest, "opacity",
+                     "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    rec = np.frombuffer(data[end:], "<f4").reshape(n, len(props))
+    np.testing.assert_array_equal(rec[:, 9:9 + 3 * K], sh.transpose(0, 2, 1).reshape(n, 3 * K))
+    np.testing.assert_array_equal(rec[:, 6:9], m.colors)
+    np.testing.assert_array_equal(rec[:, 9 + 3 * K], m.opacities)
+    np.testing.assert_array_equal(rec[:, -4:], m.quats)
+    r, splat = assert_same(reference, path)
+    assert splat
+    for name in GROUPS_ORDER:
+        np.testing.assert_array_equal(getattr(r, name), getattr(m, name))
+    for bad in (0, 4):
+        assert not api.writeSplatPlySh(str(tmp_path / "bad.ply"), m, sh, bad)

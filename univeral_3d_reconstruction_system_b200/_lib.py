@@ -100,6 +100,7 @@ SIGNATURES = {
     "u3dg_adam_destroy": (None, [_P]),
     "u3dg_init_gaussians_from_points": (C.c_int, [_F, _F, C.c_size_t, _MV]),
     "u3dg_write_splat_ply": (C.c_int, [C.c_char_p, _MV]),
+    "u3dg_write_splat_ply_sh": (C.c_int, [C.c_char_p, _MV, _F, C.c_int]),
     "u3dg_crop_model": (C.c_int, [_MV, C.POINTER(_abi.CropBox), C.c_float, _MV, C.c_size_t, _SZ]),
     "u3dg_suggest_crop_box": (C.c_int, [_MV, C.c_float, C.c_float, C.c_float, C.POINTER(_abi.CropBox)]),
     "u3dg_model_bounds": (C.c_int, [_MV, C.POINTER(_abi.CropBox)]),

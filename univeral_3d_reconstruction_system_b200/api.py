@@ -462,6 +462,18 @@ def writeSplatPly(path: str, model: GaussianModel, result: PlyResult | None = No
     return st == _abi.OK
 
 
+def writeSplatPlySh(path: str, model: GaussianModel, sh_rest: np.ndarray, degree: int,
+                    result: PlyResult | None = None) -> bool:
+    """writeSplatPly plus f_rest_* properties for SH degree 1..3 (u3dg_write_splat_ply_sh). sh_rest:
+    (n, K, 3) float32, K = (degree + 1)^2 - 1, the layout renderViewsSh takes."""
+    sh = np.ascontiguousarray(sh_rest, np.float32)
+    v = model.view()
+    st = load().u3dg_write_splat_ply_sh(str(path).encode(), C.byref(v), _abi.fptr(sh), int(degree))
+    if st != _abi.OK and result is not None:
+        result.error = load().u3dg_last_error().decode()
+    return st == _abi.OK
+
+
 def readSplatPly(path: str, result: PlyResult | None = None):
     """Returns (model or None, is_splat)."""
     L = load()

@@ -1164,6 +1164,23 @@ int u3dg_write_splat_ply(const char *path, const u3dg_model *model)
     });
 }
 
+int u3dg_write_splat_ply_sh(const char *path, const u3dg_model *model, const float *sh_rest, int degree)
+{
+    return guarded([&] {
+        if (!path)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "path is NULL");
+        requireModel(model, "model");
+        if (!sh_rest && model->count > 0)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "sh_rest is NULL");
+        if (degree < 1 || degree > 3)
+            throw StatusError(U3DG_ERR_INVALID_ARG, "SH degree must be 1..3");
+        static const float kNone = 0.0f;
+        std::string err;
+        if (!writeSplatPlyHost(path, *model, &err, sh_rest ? sh_rest : &kNone, degree))
+            throw StatusError(U3DG_ERR_IO, err);
+    });
+}
+
 int u3dg_read_splat_ply(const char *path, u3dg_model *out, size_t capacity, size_t *count, int *is_splat)
 {
     return guarded([&] {

@@ -41,8 +41,11 @@ void finishInitFromNeighbours(const float *xyz, const float *rgb, size_t n, floa
                               u3dg_model &out);
 // The same initialisation with the 27-cell neighbour search on the current GPU (bit-identical).
 void initGaussiansFromPointsDevice(const float *xyz, const float *rgb, size_t n, u3dg_model &out);
-// writeSplatPly (SplatPly.cpp:261-282).
-bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error);
+// writeSplatPly (SplatPly.cpp:261-282). With shRest (shDegree 1..3; K = (shDegree + 1)^2 - 1
+// coefficients per channel, laid out as u3dg_render_sh takes them: [i][k][channel]), the common 3DGS
+// extension: properties f_rest_0 .. f_rest_{3K-1} after f_dc_2, channel-major (f_rest_{c K + k}).
+bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error, const float *shRest = nullptr,
+                       int shDegree = 0);
 // readSplatPly (SplatPly.cpp:284-342).
 bool readSplatPlyHost(const std::string &path, HostModel &m, std::string *error, bool *isSplat);
 

@@ -413,8 +413,12 @@ bool readFile(const std::string &path, std::vector<char> &bytes, std::string *er
 
 // ---------------------------------------------------------------- public
 
-bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error)
+bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string *error, const float *shRest,
+                       int shDegree)
 {
+    if (shRest != nullptr && (shDegree < 1 || shDegree > 3))
+        return fail(error, "SH degree must be 1..3 with higher-order coefficients");
+    const size_t K = shRest ? size_t((shDegree + 1) * (shDegree + 1) - 1) : 0;
     std::ofstream out(path, std::ios::binary);
     if (!out)
         return fail(error, "Cannot write " + path);
@@ -424,12 +428,17 @@ bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string
                                          "scale_2", "rot_0",  "rot_1",   "rot_2",   "rot_3"};
     std::string head = "ply\nformat binary_little_endian 1.0\ncomment Universal 3D Reconstruction System\n";
     head += "element vertex " + std::to_string(m.count) + "\n";
-    for (const char *p : kProps)
-        head += std::string("property float ") + p + "\n";
+    for (int j = 0; j < 17; ++j) {
+        head += std::string("property float ") + kProps[j] + "\n";
+        if (j == 8) // after f_dc_2
+            for (size_t r = 0; r < 3 * K; ++r)
+                head += "property float f_rest_" + std::to_string(r) + "\n";
+    }
     head += "end_header\n";
     out.write(head.data(), std::streamsize(head.size()));
     // Records assembled in blocks of up to 64k Gaussians and written with one call per block.
-    constexpr size_t kRec = 17, kBlock = 65536;
+    const size_t kRec = 17 + 3 * K;
+    constexpr size_t kBlock = 65536;
     std::vector<float> buf;
     for (size_t first = 0; first < m.count && out; first += kBlock) {
         const size_t n = std::min(kBlock, m.count - first);
@@ -439,9 +448,13 @@ bool writeSplatPlyHost(const std::string &path, const u3dg_model &m, std::string
             float *r = &buf[j * kRec];
             std::memcpy(r, m.means + i * 3, 3 * sizeof(float));
             std::memcpy(r + 6, m.colors + i * 3, 3 * sizeof(float));
-            r[9] = m.opacities[i];
-            std::memcpy(r + 10, m.scales + i * 3, 3 * sizeof(float));
-            std::memcpy(r + 13, m.quats + i * 4, 4 * sizeof(float));
+            for (size_t c = 0; c < 3; ++c) // f_rest_{c K + k} from [i][k][c]
+                for (size_t k = 0; k < K; ++k)
+                    r[9 + c * K + k] = shRest[(i * K + k) * 3 + c];
+            float *t = r + 9 + 3 * K;
+            t[0] = m.opacities[i];
+            std::memcpy(t + 1, m.scales + i * 3, 3 * sizeof(float));
+            std::memcpy(t + 4, m.quats + i * 4, 4 * sizeof(float));
         }
         if (!hostLittleEndian())
             for (float &v : buf) {
