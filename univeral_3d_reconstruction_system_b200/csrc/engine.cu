@@ -638,6 +638,9 @@ void TrainerImpl::stepTo(int target)
     while (iteration < target && !cams.empty()) {
         if (graphEligible(target)) {
             if (pending < 0) {
+                // Record the run's graph first if it needs one: the capture executes nothing, so it
+                // overlaps the single steps still running on the device instead of following them.
+                primeGraph(target);
                 finish(); // graph runs start with no single step in flight
                 if (!graphEligible(target))
                     continue;
