@@ -236,7 +236,9 @@ __global__ void __launch_bounds__(kThreads) lossBackwardKernel(const float *rend
 }
 
 // Single block: fixed-order sum of the block partials, LossValue, PSNR and the EMA stats.
-__global__ void __launch_bounds__(kThreads) lossFinalizeKernel(const double *blockSums, int blocks, int W, int H,
+constexpr int kFinalThreads = 1024;
+
+__global__ void __launch_bounds__(kFinalThreads) lossFinalizeKernel(const double *blockSums, int blocks, int W, int H,
                                                                float lambda, DevStats *stats, int iteration,
                                                                const BinCounts *counts, float *out3, float *psnrOut,
                                                                const StepDesc *desc)
@@ -246,17 +248,35 @@ __global__ void __launch_bounds__(kThreads) lossFinalizeKernel(const double *blo
         iteration = desc->iteration + 1;
     if (counts != nullptr && counts->abortIter >= 0)
         stats = nullptr; // an aborted step leaves the statistics alone (it is replayed)
+    // The three sums over the loss blocks in a fixed order: strided per thread, a butterfly per warp,
+    // then the warps' sums in warp order (one barrier for all three).
+    __shared__ double warpSums[kFinalThreads / 32][3];
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int b = threadIdx.x; b < blocks; b += kThreads) {
+    for (int b = threadIdx.x; b < blocks; b += kFinalThreads) {
         s0 += blockSums[3 * b];
         s1 += blockSums[3 * b + 1];
         s2 += blockSums[3 * b + 2];
     }
-    s0 = blockSumDouble(s0);
-    s1 = blockSumDouble(s1);
-    s2 = blockSumDouble(s2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        warpSums[threadIdx.x >> 5][0] = s0;
+        warpSums[threadIdx.x >> 5][1] = s1;
+        warpSums[threadIdx.x >> 5][2] = s2;
+    }
+    __syncthreads();
     if (threadIdx.x != 0)
         return;
+    s0 = s1 = s2 = 0.0;
+    for (int w = 0; w < kFinalThreads / 32; ++w) {
+        s0 += warpSums[w][0];
+        s1 += warpSums[w][1];
+        s2 += warpSums[w][2];
+    }
     const size_t P = size_t(W) * H;
     const float invCount = 1.0f / float(P * 3);
     const float l1 = float(s0 * invCount);
@@ -352,7 +372,7 @@ void launchLoss(const float *render, const float *targetF, const uint8_t *target
 void launchLossFinalize(const LossScratch &ls, int width, int height, float lambda, DevStats *stats, int iteration,
                         const BinCounts *counts, float *out3, float *psnrOut, cudaStream_t s, const StepDesc *desc)
 {
-    { launchPdl(lossFinalizeKernel, 1, kThreads, 0, s, ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
+    { launchPdl(lossFinalizeKernel, 1, kFinalThreads, 0, s, ls.blockSums, ls.blocks, width, height, lambda, stats, iteration,
                                               counts, out3, psnrOut, desc); countLaunch(); }
 }
 

@@ -187,9 +187,21 @@ __global__ void __launch_bounds__(1024) blockOrderKernel(const int *tileOffsets,
         atomicAdd(&count[lengthBucket(unsigned(tileOffsets[t + 1] - tileOffsets[t]))], 1);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int b = 0; b < kOrderBuckets; ++b) {
+    if (threadIdx.x < 32) { // exclusive scan of the bucket counts: each lane owns kPer consecutive buckets
+        constexpr int kPer = (kOrderBuckets + 31) / 32;
+        const int lane = threadIdx.x, b0 = lane * kPer;
+        int own = 0;
+        for (int b = b0; b < b0 + kPer && b < kOrderBuckets; ++b)
+            own += count[b];
+        int incl = own;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        int run = incl - own;
+        for (int b = b0; b < b0 + kPer && b < kOrderBuckets; ++b) {
             cursor[b] = run;
             run += count[b];
         }
